@@ -1,0 +1,155 @@
+/* nipet_b200.h -- C ABI of the B200 reconstruction hot path for the Siemens mMR.
+ *
+ * Plain pointers and sizes only.  "dev" pointers are CUDA device (or managed)
+ * memory on the handle's device; "host" pointers are ordinary host memory.
+ * Every entry point returns an nb_status (0 = success) and never exits the
+ * process; nb_last_error() gives a message for the calling thread's last failure.
+ * Work is enqueued on the given CUDA stream (NULL = legacy default stream);
+ * nothing synchronises unless the entry point says so.
+ *
+ * Each declaration names the reference interface it replaces
+ * (paths inside the NiftyPET/NIPET tree).
+ */
+#ifndef NIPET_B200_H
+#define NIPET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  NB_OK = 0,
+  NB_ERR_ARG = 1,         /* invalid argument (null pointer, size, span, index range) */
+  NB_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  NB_ERR_NOMEM = 3,       /* device allocation failed */
+  NB_ERR_DEVICE = 4,      /* a kernel reported a device-side error (see nb_last_error) */
+  NB_ERR_UNSUPPORTED = 5, /* valid in the reference but not provided here */
+  NB_ERR_DATA = 6         /* malformed input data (e.g. list-mode stream without time tags) */
+} nb_status;
+
+/* Opaque geometry handle: device-resident LUTs, Siddon step lists and scratch. */
+typedef struct nb_geom nb_geom;
+
+int nb_version(void);
+const char *nb_strerror(int status);
+const char *nb_last_error(void);
+
+/* ---- geometry -------------------------------------------------------------------------
+ * Replaces the per-call LUT upload and transaxial table computation of
+ * prj/src/prj_module.cu:380-398 (fprj), :560-585 (bprj), prj/src/recon.cu:334-349 (osem)
+ * and prj/src/tprj.cu:174-200 (gpu_siddon_tx): tables are computed once per handle.
+ *   crs    host [ncrs][4] float   (txLUT['crs'])
+ *   s2c    host [naw][2] int16    (txLUT['s2c'])
+ *   li2rng host [nli2r][2] float  (axLUT['li2rng'])
+ *   li2sn  host [nli2r][2] int16  (axLUT['li2sn'], span-11)
+ *   li2sn1 host [nli2r][2] int16  (axLUT['li2sn1'], span-1)
+ *   li2nos host [nli2r] int8      (axLUT['li2nos'])
+ * Only the full mMR geometry is accepted (ncrs 504, naw 68516, nli2r 2074). */
+int nb_geom_create(int device, const float *crs, int ncrs, const int16_t *s2c, int naw,
+                   const float *li2rng, const int16_t *li2sn, const int16_t *li2sn1,
+                   const int8_t *li2nos, int nli2r, nb_geom **out);
+int nb_geom_destroy(nb_geom *g);
+
+/* Transaxial Siddon tables in the reference layout: tt host [naw][10] float, tv host
+ * [naw][1807] uint8.  Replaces petprj.tprj (prj/src/prj_module.cu:70-224).  Synchronous. */
+int nb_geom_tables(nb_geom *g, float *tt, uint8_t *tv);
+
+/* Voxel-read count V of a forward projection over all LORs (direct: 1 per step,
+ * oblique: 2 per step, 4 at an axial crossing), computed on the device.  Synchronous. */
+int nb_geom_count_reads(nb_geom *g, long long *reads);
+
+/* ---- projectors on the reference image layout [320][320][127] (y, x, z) ---------------
+ * nb_fprj replaces petprj.fprj (prj/src/prj_module.cu:232-425 -> gpu_fprj, prjf.cu:209-320).
+ *   sino dev [nprj][nsinos] float, overwritten; nsinos 837 (span 11) or 4084 (span 1)
+ *   im   dev [320*320*127] float
+ *   subs dev [nprj] int32 LOR indices into [0, 68516), or NULL for all 68516 LORs in order
+ *   att  0 emission (line integrals), 1 attenuation factors exp(-integral)
+ * nb_bprj replaces petprj.bprj (prj_module.cu:430-608 -> gpu_bprj, prjb.cu:190-308).
+ *   im   dev [320*320*127] float, overwritten with the back projection of sino. */
+int nb_fprj(nb_geom *g, float *sino, const float *im, const int32_t *subs, int nprj, int span,
+            int att, void *stream);
+int nb_bprj(nb_geom *g, float *im, const float *sino, const int32_t *subs, int nprj, int span,
+            void *stream);
+
+/* ---- the same projectors on the internal "col128" layout -------------------------------
+ * col128: nimg images of [320*320][128] float, column-major in z with even z in slots
+ * [0,64), odd z in [64,127) and slot 127 zero.  nb_bprj_col128 ADDS into im128.
+ * These are the forms the OSEM and batched paths use (no layout conversion). */
+int nb_fprj_col128(nb_geom *g, float *sino, const float *im128, const int32_t *subs, int nprj,
+                   int span, int att, void *stream);
+int nb_bprj_col128(nb_geom *g, float *im128, const float *sino, const int32_t *subs, int nprj,
+                   int span, void *stream);
+int nb_im_to_col128(float *im128, const float *im, int nimg, void *stream);
+int nb_col128_to_im(float *im, const float *im128, int nimg, void *stream);
+
+/* Synchronise `stream` and report (then clear) any device-side error a kernel of this
+ * handle raised.  Synchronous. */
+int nb_geom_check(nb_geom *g, void *stream);
+
+/* ---- sinogram layout (src/scanner_0.cu:94-241, mmr_auxe.rgaps / pgaps) -----------------
+ * nb_remgaps: Siemens [snno][252*344] -> gap-free [68516][snno] (d_remgaps);
+ * nb_putgaps: gap-free [68516][snno] -> Siemens [snno][252*344], gaps set to 0 (d_putgaps).
+ *   aw2ali dev [68516] int32 (txLUT['aw2ali']).  The _u16 forms move uint16 counts. */
+int nb_remgaps(float *sng, const float *sino, int snno, const int32_t *aw2ali, void *stream);
+int nb_remgaps_u16(uint16_t *sng, const uint16_t *sino, int snno, const int32_t *aw2ali,
+                   void *stream);
+int nb_putgaps(float *sino, const float *sng, int snno, const int32_t *aw2ali, void *stream);
+
+/* ---- OSEM (prj/src/recon.cu:318-521, petprj.osem prj_module.cu:613-839) --------------
+ * nb_osem_rs: rs = (rsng + ssng) / (asng * nsng), 0 where |asng*nsng| < 1e-6
+ *   (recon.cu:381-398), all dev [n] float; ssng may be NULL (zero scatter).
+ * nb_osem_subset: one fused OSEM sub-iteration on col128 images, replacing the
+ *   per-subset rec_fprj / sneladd / sneldiv / rec_bprj / eldiv0 / elmsk sequence
+ *   (recon.cu:459-497):
+ *     img128 dev col128 image, updated in place: img = msk ? img * (bimg/sens) : 0
+ *     bimg128 dev col128 scratch image (zeroed by the call)
+ *     sens128 dev col128 sensitivity image of this subset
+ *     msk128 dev col128 uint8 mask (0 outside the reconstruction cylinder)
+ *     psng dev [68516][837] uint16 prompts; rs dev [68516][837] float from nb_osem_rs
+ *     subs dev [nprj] int32 LORs of the subset. */
+int nb_osem_rs(float *rs, const float *rsng, const float *ssng, const float *asng,
+               const float *nsng, size_t n, void *stream);
+int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens128,
+                   const uint8_t *msk128, const uint16_t *psng, const float *rs,
+                   const int32_t *subs, int nprj, void *stream);
+
+/* ---- list-mode histogramming (lm/src/lmproc.cu:12-230, hst.cu:37-528, lmaux.cu:17-270) -
+ * nb_lm_plan replaces getLMinfo + modifyLMinfo: the chunk plan of a list-mode stream
+ * (host [ele] int32 words), chunks cut at time tags with t % 100 ms == 0, and the time
+ * window [t0, t1) in seconds (t0 == t1: whole stream).  Arrays have capacity `cap`.
+ * Returns the number of chunks in *nchnk. */
+int nb_lm_plan(const int32_t *lm, int64_t ele, int t0, int t1, int cap, int64_t *atag,
+               int *ele4chnk, int *ele4thrd, int *nchnk, int *toff, int *nitag, int *tstart,
+               int *tstop);
+
+/* nb_hist replaces gpu_hst (hst.cu:347-528) + the lmproc unpack (lmproc.cu:156-193):
+ * histograms the dev stream `lm` (the whole file, word 0 = file word 0) with the plan
+ * from nb_lm_plan (host arrays), for `nrep` bootstrap replicates rep0..rep0+nrep-1.
+ *   span 1, 11 or 0 (SSRB); btp 0 none, 1 non-parametric, 2 parametric (Poisson(btprt))
+ *   seed: bootstrap stream key (Philox4x32-10; counter = (word index, replicate, draw))
+ * Outputs (dev, ZEROED BY THE CALLER, accumulated):
+ *   psino [nrep][nbins] uint32 packed prompts (low 16 bits) / delayeds (high 16 bits)
+ *   ssrb [nrep][127*86688] uint32, phc/dhc [nrep][nitag] uint32, zR/zM [nrep][nitag] int32,
+ *   pvs [nrep][sne] uint32, fan [nrep][64*504] uint32, bck [nrep][2*224*nitag] uint32
+ *   (nbins: 354033792 span 1, 72557856 span 11, 11009376 span 0;
+ *    sne = ceil(min(nitag,5400)/4)*127*344 as lmproc.cu:60-63)
+ *   sn1_sn11, sn1_ssrb, sn1_rno, s2cF: host LUTs (axLUT/txLUT, int16). */
+int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag, const int *ele4chnk,
+            const int *ele4thrd, int toff, int nitag, int tstart, int tstop, int span, int btp,
+            double btprt, uint64_t seed, int rep0, int nrep, const int16_t *sn1_sn11,
+            const int16_t *sn1_ssrb, const int16_t *sn1_rno, const int16_t *s2cF,
+            uint32_t *psino, uint32_t *ssrb, uint32_t *phc, uint32_t *dhc, int32_t *zR,
+            int32_t *zM, uint32_t *pvs, uint32_t *fan, uint32_t *bck, void *stream);
+
+/* Split packed sinograms: psn = w & 0xFFFF, dsn = w >> 16 (lmproc.cu:162-168), and the
+ * prompt/delayed totals (host, may be NULL).  Synchronous. */
+int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t *dsn,
+                   unsigned long long *psum, unsigned long long *dsum, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NIPET_B200_H */

@@ -1,0 +1,506 @@
+// nb_hist.cu -- list-mode histogramming of Siemens mMR 32-bit event words.
+//
+// Reference semantics: lm/src/hst.cu:37-244 (kernel hst), lm/src/lmaux.cu:17-270
+// (chunk plan getLMinfo / modifyLMinfo), lm/src/lmproc.cu:156-193 (unpack).
+//
+// Bit-exactness with the reference comes from reproducing its work decomposition, not
+// its launch shape: the reference cuts the stream into chunks ending at 100-ms time
+// tags and each chunk into 2560 thread slices; a slice's events before its first time
+// tag are attributed to that tag's second, and time tags are honoured only while the
+// slice's current second is inside the frame window.  Here one warp processes one slice
+// (32 consecutive words per step, coalesced), carrying the slice's current second
+// across steps, so head curves, centre of mass and projection views match bit for bit.
+// All counters are uint32 sums (order independent, wrap-around like the reference);
+// per-second counters are warp-aggregated before their atomic.
+//
+// Bootstrap: the reference draws from clock()-seeded curand states; here every draw is
+// Philox4x32-10 (Salmon et al., SC'11) keyed by the 64-bit seed, with counter
+// (word index, replicate, draw), so replicates are reproducible and independent of
+// the launch shape.  btp=2 draws N ~ Poisson(btprt) per word by integer inverse CDF
+// (events with N = 0 or N >= 32 are dropped as in the reference); btp=1 replaces each
+// event word by a uniformly drawn event word of the same slice (at most 64 draws).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "nb_internal.cuh"
+
+#define NB_TOTHRDS 2560
+#define NB_ELECHNK (402653184 / 32)
+#define NB_ITIME 1000
+#define NB_BTPTIME 100
+#define NB_MXNITAG 5400
+#define NB_NBUCKTS 224
+
+struct HistLUT {
+  int16_t sn1_sn11[NB_NSN1];
+  int16_t sn1_ssrb[NB_NSN1];
+  int16_t sn1_rno[2 * NB_NSN1];
+};
+
+struct HistArgs {
+  const int32_t *lm;
+  const int64_t *atag;   // chunk starts [nchnk]
+  const int *e4c;        // words per chunk
+  const int *e4t;        // words per thread slice
+  int nchnk;
+  int toff, nitag, tstart, tstop, span, btp;
+  uint64_t seed;
+  int rep0, nrep;
+  const HistLUT *lut;
+  const short2 *s2cF;
+  uint64_t thr[32];      // Poisson inverse-CDF thresholds (2^32 scaled)
+  size_t nbins, sne;
+  uint32_t *psino, *ssrb, *phc, *dhc, *pvs, *fan, *bck;
+  int32_t *zR, *zM;
+};
+
+static __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+static __device__ __forceinline__ uint32_t boot_draw(uint64_t seed, int rep, uint64_t gidx,
+                                                     uint32_t stream) {
+  uint32_t c[4] = {(uint32_t)gidx, (uint32_t)(gidx >> 32), (uint32_t)rep, stream};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  return c[0];
+}
+
+__global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
+  __shared__ HistLUT slut;
+  for (int i = threadIdx.x; i < (int)(sizeof(HistLUT) / 4); i += blockDim.x)
+    reinterpret_cast<int *>(&slut)[i] = reinterpret_cast<const int *>(a.lut)[i];
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int nwarps_total = (gridDim.x * blockDim.x) >> 5;
+  const int nslices = a.nchnk * NB_TOTHRDS;
+  for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices; sl += nwarps_total) {
+    const int n = sl / NB_TOTHRDS, idx = sl - n * NB_TOTHRDS;
+    const int64_t off = a.atag[n];
+    const int elm = a.e4c[n], e4t = a.e4t[n];
+    int64_t s0, s1;
+    if (idx == NB_TOTHRDS - 1) {
+      s1 = off + elm;
+      s0 = off + (int64_t)(NB_TOTHRDS - 1) * e4t;
+    } else {
+      s1 = off + (int64_t)(idx + 1) * e4t;
+      s0 = off + (int64_t)idx * e4t;
+    }
+    if (s1 > off + elm) s1 = off + elm;
+    if (s0 >= s1) continue;
+
+    // initial second: first time tag in [s0, s1-1) (hst.cu:84-100)
+    int cur = a.nitag, curu = 0;
+    for (int64_t base = s0; base < s1 - 1; base += 32) {
+      const int64_t i = base + lane;
+      const int wd = (i < s1 - 1) ? a.lm[i] : 0;
+      const unsigned m = __ballot_sync(0xffffffffu, (wd >> 29) == -4);
+      if (m) {
+        const int src = __ffs(m) - 1;
+        const int tv = (__shfl_sync(0xffffffffu, wd, src) & 0x1fffffff) - a.toff;
+        cur = tv / NB_ITIME;
+        curu = tv - cur * NB_ITIME;
+        break;
+      }
+    }
+    const int64_t slen = s1 - s0;
+
+    for (int64_t base = s0; base < s1; base += 32) {
+      // a slice is dead once its current second leaves the window (hst.cu:135)
+      if (!(cur >= a.tstart && cur < a.tstop)) break;
+      const int64_t i = base + lane;
+      const bool inb = i < s1;
+      const int word0 = inb ? a.lm[i] : 0;
+      const bool istag = inb && (word0 >> 29) == -4;
+      const unsigned tmask = __ballot_sync(0xffffffffu, istag);
+      const int tval = istag ? (word0 & 0x3fffffff) - a.toff : 0;
+      const int titag = tval / NB_ITIME;
+      // the second in force when this word is processed
+      const unsigned before = tmask & ((1u << lane) - 1u);
+      const int srcl = before ? 31 - __clz(before) : -1;
+      const int my_itag_t = __shfl_sync(0xffffffffu, titag, srcl < 0 ? 0 : srcl);
+      const int my_itagu_t = __shfl_sync(0xffffffffu, tval - titag * NB_ITIME, srcl < 0 ? 0 : srcl);
+      const int itag = srcl < 0 ? cur : my_itag_t;
+      const int itagu = srcl < 0 ? curu : my_itagu_t;
+      const bool okw = itag >= a.tstart && itag < a.tstop;
+      const unsigned bad = __ballot_sync(0xffffffffu, inb && !okw);
+      const bool live = inb && (bad == 0 || lane < __ffs(bad) - 1);
+      // carry the second to the next step
+      const unsigned livetags = tmask & __ballot_sync(0xffffffffu, live);
+      if (livetags) {
+        const int last = 31 - __clz(livetags);
+        cur = __shfl_sync(0xffffffffu, titag, last);
+        curu = __shfl_sync(0xffffffffu, tval - titag * NB_ITIME, last);
+      }
+      if (bad) cur = -2147483647;  // dead from the first out-of-window word on
+
+      // ---- singles (hst.cu:215-235), in word order within the warp ----
+      {
+        const bool issgl = live && (word0 >> 29) == -3;
+        unsigned sm = __ballot_sync(0xffffffffu, issgl);
+        while (sm) {
+          const int L = __ffs(sm) - 1;
+          sm &= sm - 1;
+          if (lane == L) {
+            const unsigned ibck = (unsigned)((word0 & 0x1fffffff) >> 19);
+            if (ibck < NB_NBUCKTS) {
+              for (int r = 0; r < a.nrep; r++) {
+                uint32_t *bk = a.bck + (size_t)r * 2 * NB_NBUCKTS * a.nitag;
+                const size_t b0 = ibck + (size_t)NB_NBUCKTS * itag;
+                const size_t b1 = b0 + (size_t)NB_NBUCKTS * a.nitag;
+                atomicAdd(bk + b0, (uint32_t)(word0 & 0x0007ffff) << 3);
+                const uint32_t prev =
+                    atomicAdd(bk + b1, (uint32_t)((word0 & 0x0007ffff) > 0) << 30);
+                const uint32_t now = prev + ((uint32_t)((word0 & 0x0007ffff) > 0) << 30);
+                atomicAdd(bk + b1, now == 0 ? (uint32_t)itagu : (uint32_t)itagu << 10);
+              }
+            }
+          }
+          __syncwarp();
+        }
+      }
+
+      // ---- events, per replicate ----
+      for (int r = 0; r < a.nrep; r++) {
+        const int rep = a.rep0 + r;
+        int word = word0;
+        uint32_t N = 1;
+        if (a.btp == 1) {
+          if (live && word0 > 0) {
+            bool got = false;
+            for (uint32_t jd = 0; jd < 64 && !got; jd++) {
+              const uint32_t x = boot_draw(a.seed, rep, (uint64_t)i, 1 + jd);
+              const int64_t bi = (int64_t)(((uint64_t)x * (uint64_t)slen) >> 32);
+              const int cand = a.lm[s0 + bi];
+              if (cand > 0) {
+                word = cand;
+                got = true;
+              }
+            }
+            if (!got) N = 0;
+          }
+        } else if (a.btp == 2) {
+          const uint32_t x = boot_draw(a.seed, rep, (uint64_t)i, 0);
+          uint32_t k = 0;
+#pragma unroll
+          for (int q = 0; q < 32; q++) k += (uint64_t)x >= a.thr[q] ? 1u : 0u;
+          N = k;
+        }
+        const bool ev = live && word > 0 && N > 0 && N < 32;
+        const int val = word & 0x3fffffff;
+        int si = val / NB_NSBINANG;
+        const bool ok = ev && si < NB_NSN1;
+        uint32_t p_n = 0, d_n = 0, zr = 0;
+        if (ok) {
+          const int aw = val - si * NB_NSBINANG;
+          const int an = aw / NB_NSBINS;
+          const int w = aw - an * NB_NSBINS;
+          const int si11 = slut.sn1_sn11[si];
+          const int sis = slut.sn1_ssrb[si];
+          size_t addr;
+          if (a.span == 1)
+            addr = (size_t)val;
+          else if (a.span == 11)
+            addr = (size_t)si11 * NB_NSBINANG + aw;
+          else
+            addr = (size_t)sis * NB_NSBINANG + aw;
+          uint32_t *ps = a.psino + (size_t)r * a.nbins;
+          if ((word >> 30) == 1) {
+            p_n = N;
+            zr = (uint32_t)sis;
+            atomicAdd(a.ssrb + (size_t)r * NB_SEG0 * NB_NSBINANG + (size_t)sis * NB_NSBINANG + aw,
+                      N);
+            atomicAdd(ps + addr, N);
+            if ((an == 0 || an == 126) && itag < NB_MXNITAG)
+              atomicAdd(a.pvs + (size_t)r * a.sne + (size_t)(itag >> 2) * NB_SEG0 * NB_NSBINS +
+                            sis * NB_NSBINS + w,
+                        N << ((an == 126) * 8));
+          } else {
+            d_n = N;
+            atomicAdd(ps + addr, N << 16);
+            const short2 cc = a.s2cF[an + NB_NSANGLES * w];
+            uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
+            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * si] + cc.x, N);
+            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * si + 1] + cc.y, N);
+          }
+        }
+        // per-second counters: one atomic per distinct second in the warp
+        const unsigned act = __ballot_sync(0xffffffffu, ok);
+        if (act) {
+          const unsigned grp = __match_any_sync(0xffffffffu, ok ? itag : -1);
+          if (ok) {
+            const uint32_t sp = __reduce_add_sync(grp, p_n);
+            const uint32_t sd = __reduce_add_sync(grp, d_n);
+            const uint32_t sz = __reduce_add_sync(grp, zr);
+            if (lane == __ffs(grp) - 1) {
+              const size_t o = (size_t)r * a.nitag + itag;
+              if (sp) {
+                atomicAdd(a.phc + o, sp);
+                atomicAdd((uint32_t *)a.zM + o, sp);
+                atomicAdd((uint32_t *)a.zR + o, sz);
+              }
+              if (sd) atomicAdd(a.dhc + o, sd);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// host: chunk plan (lmaux.cu:17-270)
+// ---------------------------------------------------------------------------------------
+extern "C" int nb_lm_plan(const int32_t *lm, int64_t ele, int t0, int t1, int cap, int64_t *atag,
+                          int *ele4chnk, int *ele4thrd, int *nchnk, int *toff, int *nitag,
+                          int *tstart, int *tstop) {
+  NB_REQUIRE(lm && atag && ele4chnk && ele4thrd && nchnk && toff && nitag && tstart && tstop,
+             "nb_lm_plan: NULL argument");
+  NB_REQUIRE(ele > 0, "nb_lm_plan: empty stream");
+  int64_t i0 = -1, i1 = -1;
+  for (int64_t i = 0; i < ele; i++)
+    if ((lm[i] >> 29) == -4) {
+      i0 = i;
+      break;
+    }
+  for (int64_t i = ele - 1; i >= 0; i--)
+    if ((lm[i] >> 29) == -4) {
+      i1 = i;
+      break;
+    }
+  if (i0 < 0) {
+    nb_set_error_msg("nb_lm_plan: no time tag in the list-mode stream");
+    return NB_ERR_DATA;
+  }
+  const int first = lm[i0] & 0x1fffffff, last = lm[i1] & 0x1fffffff;
+  if (!(first < last)) {
+    nb_set_error_msg("nb_lm_plan: first time tag %d is not before the last %d", first, last);
+    return NB_ERR_DATA;
+  }
+  const int tof = first;
+  const int nit = ((last - tof) + NB_ITIME - 1) / NB_ITIME;
+  std::vector<int64_t> A(1, 0), Bt(1, 0);
+  std::vector<int> E, ET;
+  while ((ele - A.back()) > (int64_t)NB_ELECHNK) {
+    const int64_t prev = A.back();
+    int64_t found = -1;
+    for (int64_t pos = prev + NB_ELECHNK - 1; pos > prev; pos--) {
+      const int wd = lm[pos];
+      if ((wd >> 29) == -4 && ((wd & 0x1fffffff) % NB_BTPTIME) == 0) {
+        found = pos;
+        break;
+      }
+    }
+    if (found < 0) {
+      nb_set_error_msg("nb_lm_plan: no 100-ms time tag within %d words after word %lld",
+                       NB_ELECHNK, (long long)prev);
+      return NB_ERR_DATA;
+    }
+    Bt.push_back((int64_t)((lm[found] & 0x1fffffff) - tof));
+    A.push_back(found);
+    E.push_back((int)(found - prev));
+    ET.push_back((int)((found - prev + NB_TOTHRDS - 1) / NB_TOTHRDS));
+  }
+  Bt.push_back((int64_t)(last - tof + 1));
+  const int64_t prev = A.back();
+  A.push_back(ele);
+  E.push_back((int)(ele - prev));
+  ET.push_back((int)((ele - prev + NB_TOTHRDS - 1) / NB_TOTHRDS));
+  const int nch = (int)E.size();
+  int ts = t0, te = t1;
+  if (ts == te) {
+    ts = 0;
+    te = nit;
+  }
+  int n0 = -1, n1 = -1, newn = 0;
+  for (int n = 0; n < nch; n++)
+    if (ts <= (Bt[n + 1] / NB_ITIME) && (Bt[n] / NB_ITIME) < te) {
+      if (n0 == -1) n0 = n;
+      n1 = n;
+      newn++;
+    }
+  if (newn + 1 > cap) {
+    nb_set_error_msg("nb_lm_plan: capacity %d too small for %d chunks", cap, newn);
+    return NB_ERR_ARG;
+  }
+  int nn = 0;
+  if (newn > 0) {
+    for (int n = n0; n <= n1; n++) {
+      atag[nn] = A[n];
+      ele4chnk[nn] = E[n];
+      ele4thrd[nn] = ET[n];
+      nn++;
+    }
+    atag[nn] = A[n1 + 1];
+  }
+  *nchnk = newn;
+  *toff = tof;
+  *nitag = nit;
+  *tstart = ts;
+  *tstop = te;
+  return NB_OK;
+}
+
+static void poisson_thresholds(double lam, uint64_t thr[32]) {
+  double pmf = exp(-lam), cdf = 0;
+  for (int n = 0; n < 32; n++) {
+    if (n > 0) pmf = pmf * lam / (double)n;
+    cdf += pmf;
+    const double t = ceil(cdf * 4294967296.0);
+    thr[n] = t >= 4294967296.0 ? 4294967296ull : (uint64_t)t;
+  }
+}
+
+extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag,
+                       const int *ele4chnk, const int *ele4thrd, int toff, int nitag, int tstart,
+                       int tstop, int span, int btp, double btprt, uint64_t seed, int rep0,
+                       int nrep, const int16_t *sn1_sn11, const int16_t *sn1_ssrb,
+                       const int16_t *sn1_rno, const int16_t *s2cF, uint32_t *psino,
+                       uint32_t *ssrb, uint32_t *phc, uint32_t *dhc, int32_t *zR, int32_t *zM,
+                       uint32_t *pvs, uint32_t *fan, uint32_t *bck, void *stream) {
+  NB_REQUIRE(lm && atag && ele4chnk && ele4thrd, "nb_hist: NULL stream or plan");
+  NB_REQUIRE(sn1_sn11 && sn1_ssrb && sn1_rno && s2cF, "nb_hist: NULL LUT");
+  NB_REQUIRE(psino && ssrb && phc && dhc && zR && zM && pvs && fan && bck,
+             "nb_hist: NULL output");
+  NB_REQUIRE(span == 0 || span == 1 || span == 11, "nb_hist: span must be 0, 1 or 11");
+  NB_REQUIRE(btp >= 0 && btp <= 2, "nb_hist: btp must be 0, 1 or 2");
+  NB_REQUIRE(nrep >= 1 && nitag > 0 && nchnk >= 0, "nb_hist: bad sizes");
+  NB_REQUIRE(!(btp == 2 && !(btprt > 0)), "nb_hist: btprt must be > 0");
+  for (int n = 0; n < nchnk; n++) {
+    NB_REQUIRE(atag[n] >= 0 && ele4chnk[n] >= 0 && atag[n] + ele4chnk[n] <= ele,
+               "nb_hist: chunk outside the stream");
+    NB_REQUIRE(ele4thrd[n] >= 0, "nb_hist: bad slice length");
+  }
+  for (int i = 0; i < NB_NSN1; i++)
+    NB_REQUIRE(sn1_sn11[i] >= 0 && sn1_sn11[i] < NB_NSN11 && sn1_ssrb[i] >= 0 &&
+                   sn1_ssrb[i] < NB_SEG0 && sn1_rno[2 * i] >= 0 && sn1_rno[2 * i] < NB_NRINGS &&
+                   sn1_rno[2 * i + 1] >= 0 && sn1_rno[2 * i + 1] < NB_NRINGS,
+               "nb_hist: axial LUT out of range");
+  if (nchnk == 0) return NB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+
+  HistArgs a{};
+  a.lm = lm;
+  a.nchnk = nchnk;
+  a.toff = toff;
+  a.nitag = nitag;
+  a.tstart = tstart;
+  a.tstop = tstop;
+  a.span = span;
+  a.btp = btp;
+  a.seed = seed;
+  a.rep0 = rep0;
+  a.nrep = nrep;
+  poisson_thresholds(btp == 2 ? btprt : 1.0, a.thr);
+  a.nbins = span == 1 ? 354033792ull : (span == 11 ? 72557856ull : (size_t)NB_SEG0 * NB_NSBINANG);
+  const int tn = nitag > NB_MXNITAG ? NB_MXNITAG : nitag;
+  a.sne = (size_t)((tn + 3) / 4) * NB_SEG0 * NB_NSBINS;
+  a.psino = psino;
+  a.ssrb = ssrb;
+  a.phc = phc;
+  a.dhc = dhc;
+  a.zR = zR;
+  a.zM = zM;
+  a.pvs = pvs;
+  a.fan = fan;
+  a.bck = bck;
+
+  // small device-side tables, stream-ordered
+  HistLUT hl;
+  memcpy(hl.sn1_sn11, sn1_sn11, sizeof(hl.sn1_sn11));
+  memcpy(hl.sn1_ssrb, sn1_ssrb, sizeof(hl.sn1_ssrb));
+  memcpy(hl.sn1_rno, sn1_rno, sizeof(hl.sn1_rno));
+  const size_t plan_bytes = (size_t)nchnk * (sizeof(int64_t) + 2 * sizeof(int));
+  const size_t s2c_bytes = (size_t)NB_NSBINANG * sizeof(short2);
+  const size_t tot = sizeof(HistLUT) + s2c_bytes + plan_bytes + 64;
+  unsigned char *d = nullptr;
+  NB_CUDA(cudaMallocAsync((void **)&d, tot, s));
+  std::vector<unsigned char> h(tot);
+  size_t o = 0;
+  memcpy(&h[o], &hl, sizeof(HistLUT));
+  a.lut = (const HistLUT *)(d + o);
+  o += sizeof(HistLUT);
+  memcpy(&h[o], s2cF, s2c_bytes);
+  a.s2cF = (const short2 *)(d + o);
+  o += s2c_bytes;
+  o = (o + 15) & ~(size_t)15;
+  memcpy(&h[o], atag, sizeof(int64_t) * nchnk);
+  a.atag = (const int64_t *)(d + o);
+  o += sizeof(int64_t) * nchnk;
+  memcpy(&h[o], ele4chnk, sizeof(int) * nchnk);
+  a.e4c = (const int *)(d + o);
+  o += sizeof(int) * nchnk;
+  memcpy(&h[o], ele4thrd, sizeof(int) * nchnk);
+  a.e4t = (const int *)(d + o);
+  o += sizeof(int) * nchnk;
+  cudaError_t e = cudaMemcpyAsync(d, h.data(), o, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nslices = nchnk * NB_TOTHRDS;
+    int blocks = (nslices + 7) / 8;
+    if (blocks > nsm * 8) blocks = nsm * 8;
+    k_hist<<<blocks, 256, 0, s>>>(a);
+    e = cudaGetLastError();
+  }
+  // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go
+  cudaFreeAsync(d, s);
+  if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist", __FILE__, __LINE__);
+  return NB_OK;
+}
+
+__global__ void k_unpack(const uint32_t *__restrict__ p, size_t n, uint16_t *__restrict__ psn,
+                         uint16_t *__restrict__ dsn, unsigned long long *sums) {
+  unsigned long long ps = 0, ds = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t w = p[i];
+    const uint16_t a = (uint16_t)(w & 0xFFFF), b = (uint16_t)(w >> 16);
+    if (psn) psn[i] = a;
+    if (dsn) dsn[i] = b;
+    ps += a;
+    ds += b;
+  }
+  for (int o = 16; o; o >>= 1) {
+    ps += __shfl_down_sync(0xffffffffu, ps, o);
+    ds += __shfl_down_sync(0xffffffffu, ds, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&sums[0], ps);
+    atomicAdd(&sums[1], ds);
+  }
+}
+
+extern "C" int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t *dsn,
+                              unsigned long long *psum, unsigned long long *dsum, void *stream) {
+  NB_REQUIRE(psino != nullptr, "nb_hist_unpack: NULL input");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned long long *d = nullptr;
+  NB_CUDA(cudaMallocAsync((void **)&d, 2 * sizeof(unsigned long long), s));
+  cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), s);
+  k_unpack<<<1184, 256, 0, s>>>(psino, nbins, psn, dsn, d);
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(d, s);
+  if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist_unpack", __FILE__, __LINE__);
+  if (psum) *psum = h[0];
+  if (dsum) *dsum = h[1];
+  return NB_OK;
+}

@@ -1,0 +1,130 @@
+"""Device plumbing for the drop-in operators: device arrays, streams and the cached
+geometry handle.  PyTorch supplies device memory and streams; every computation on
+these arrays is a kernel of `libnipet_b200.so`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+
+__all__ = ['Geometry', 'get_geometry', 'to_device', 'dev_ptr', 'stream_ptr', 'device_of']
+
+
+def device_of(Cnt: dict | None = None, device=None) -> torch.device:
+    if device is not None:
+        return torch.device(device)
+    idx = int(Cnt.get('DEVID', 0)) if Cnt else 0
+    return torch.device('cuda', idx)
+
+
+def stream_ptr(device: torch.device) -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def dev_ptr(t: torch.Tensor) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+_NP2TORCH = {np.dtype('float32'): torch.float32, np.dtype('float64'): torch.float64,
+             np.dtype('int32'): torch.int32, np.dtype('int16'): torch.int16,
+             np.dtype('uint16'): torch.uint16, np.dtype('uint8'): torch.uint8,
+             np.dtype('bool'): torch.bool, np.dtype('int64'): torch.int64,
+             np.dtype('uint32'): torch.uint32, np.dtype('int8'): torch.int8}
+
+
+def to_device(x, dtype, device: torch.device, copy: bool = False) -> torch.Tensor:
+    """Contiguous device tensor view (or copy) of a numpy array, torch tensor, or any
+    object exposing `__cuda_array_interface__` / DLPack."""
+    tdt = _NP2TORCH[np.dtype(dtype)]
+    if isinstance(x, torch.Tensor):
+        t = x
+    elif isinstance(x, np.ndarray):
+        t = torch.from_numpy(np.ascontiguousarray(x))
+    elif hasattr(x, '__cuda_array_interface__') or hasattr(x, '__dlpack__'):
+        t = torch.as_tensor(x, device=device)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(x)))
+    t = t.to(device=device, dtype=tdt, non_blocking=False)
+    if not t.is_contiguous():
+        t = t.contiguous()
+    elif copy:
+        t = t.clone()
+    return t
+
+
+class Geometry:
+    """Device-resident mMR geometry (nb_geom handle): Siddon step lists built once."""
+
+    def __init__(self, txLUT: dict, axLUT: dict, device: torch.device):
+        lib = _lib.load()
+        self.device = torch.device(device)
+        self._keep = (
+            np.ascontiguousarray(txLUT['crs'], dtype=np.float32),
+            np.ascontiguousarray(txLUT['s2c'], dtype=np.int16),
+            np.ascontiguousarray(axLUT['li2rng'], dtype=np.float32),
+            np.ascontiguousarray(axLUT['li2sn'], dtype=np.int16),
+            np.ascontiguousarray(axLUT['li2sn1'], dtype=np.int16),
+            np.ascontiguousarray(axLUT['li2nos'], dtype=np.int8))
+        crs, s2c, li2rng, li2sn, li2sn1, li2nos = self._keep
+        torch.cuda.init()
+        h = C.c_void_p()
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        _lib.check(lib.nb_geom_create(self.device.index or 0, p(crs), crs.shape[0], p(s2c),
+                                      s2c.shape[0], p(li2rng), p(li2sn), p(li2sn1), p(li2nos),
+                                      li2rng.shape[0], C.byref(h)))
+        self.handle = h
+        self.naw = s2c.shape[0]
+        self.aw2ali = to_device(txLUT['aw2ali'], np.int32, self.device)
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            self._lib.nb_geom_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self):
+        """Synchronise the current stream and raise on any device-side error."""
+        _lib.check(self._lib.nb_geom_check(self.handle, stream_ptr(self.device)))
+
+    def tables(self):
+        tt = np.zeros((self.naw, 10), dtype=np.float32)
+        tv = np.zeros((self.naw, 1807), dtype=np.uint8)
+        _lib.check(self._lib.nb_geom_tables(self.handle, tt.ctypes.data_as(C.c_void_p),
+                                            tv.ctypes.data_as(C.c_void_p)))
+        return tt, tv
+
+    def count_reads(self) -> int:
+        v = C.c_longlong()
+        _lib.check(self._lib.nb_geom_count_reads(self.handle, C.byref(v)))
+        return v.value
+
+
+_CACHE: dict = {}
+_LOCK = threading.Lock()
+
+
+def get_geometry(txLUT: dict, axLUT: dict, device: torch.device) -> Geometry:
+    """The geometry handle for these LUTs on `device` (built on first use, then cached --
+    the reference rebuilds its tables on every call)."""
+    key = (str(device), id(txLUT['crs']), id(txLUT['s2c']), id(axLUT['li2rng']),
+           id(axLUT['li2sn']), id(axLUT['li2sn1']), id(axLUT['li2nos']))
+    with _LOCK:
+        g = _CACHE.get(key)
+        if g is None:
+            g = Geometry(txLUT, axLUT, device)
+            # keep the LUT objects alive so their ids stay unique while cached
+            _CACHE[key] = g
+            g._lut_refs = (txLUT['crs'], txLUT['s2c'], axLUT['li2rng'], axLUT['li2sn'],
+                           axLUT['li2sn1'], axLUT['li2nos'])
+        return g

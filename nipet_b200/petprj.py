@@ -1,0 +1,179 @@
+"""Drop-in for NIPET's `petprj` CUDA extension (`prj/src/prj_module.cu:37-43`):
+`tprj`, `fprj`, `bprj`, `osem`, with the same argument names, order and in-place
+output semantics, running on `libnipet_b200.so`.
+
+Arrays may be numpy (host; copied to the device and back like the reference's
+per-call transfers) or CUDA tensors / `__cuda_array_interface__` objects (used in place).
+Errors raise Python exceptions instead of exiting the process.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import dev_ptr, device_of, get_geometry, stream_ptr, to_device
+
+__all__ = ['tprj', 'fprj', 'bprj', 'osem', 'nsinos_of', 'NLI2R', 'NAW']
+
+NAW = 68516
+NLI2R = 2074
+IMG_SHAPE = (320, 320, 127)
+COL128 = 320 * 320 * 128
+
+
+def nsinos_of(Cnt: dict) -> int:
+    span = Cnt['SPN']
+    if span == 11:
+        return 837
+    if span == 1:
+        if Cnt.get('RNG_STRT', 0) != 0 or Cnt.get('RNG_END', 64) != 64:
+            raise NotImplementedError('reduced axial ring ranges (span-1 RNG_STRT/RNG_END) are '
+                                      'not provided by nipet_b200')
+        return 4084
+    raise ValueError(f'unsupported span {span} (the projectors support 1 and 11)')
+
+
+def _subs_arg(subs, device):
+    s = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs).reshape(-1)
+    if s.size == 0 or s[0] < 0:
+        return None, NAW
+    if s.min() < 0 or s.max() >= NAW:
+        raise ValueError('subset LOR index out of range [0, 68516)')
+    return to_device(s.astype(np.int32), np.int32, device), s.size
+
+
+def _writeback(dst, src: torch.Tensor):
+    """Copy a device result into the caller's output array in place."""
+    if isinstance(dst, torch.Tensor):
+        if dst.data_ptr() != src.data_ptr():
+            dst.copy_(src.reshape(dst.shape))
+    elif isinstance(dst, np.ndarray):
+        np.copyto(dst, src.reshape(dst.shape).cpu().numpy().astype(dst.dtype, copy=False))
+    elif hasattr(dst, '__cuda_array_interface__'):
+        torch.as_tensor(dst, device=src.device).copy_(src.reshape(tuple(dst.shape)))
+    else:
+        raise TypeError(f'unsupported output array type {type(dst)}')
+
+
+def tprj(sino, im, tv, tt, txLUT, cnst):
+    """Transaxial Siddon tables into `tv` (uint8 [Naw*1807]) and `tt` (float32 [Naw*10]),
+    as `petprj.tprj` (`prj_module.cu:70-224`).  `sino`/`im` are unused, as in the
+    reference's table-only path."""
+    dev = device_of(cnst)
+    axLUT = cnst.get('_axLUT') if isinstance(cnst, dict) else None
+    if axLUT is None:
+        from .geometry import axial_lut
+        axLUT = axial_lut(cnst)
+    g = get_geometry(txLUT, axLUT, dev)
+    t_tt, t_tv = g.tables()
+    np.copyto(np.asarray(tt).reshape(-1), t_tt.reshape(-1).astype(np.asarray(tt).dtype))
+    np.copyto(np.asarray(tv).reshape(-1), t_tv.reshape(-1).astype(np.asarray(tv).dtype))
+
+
+def fprj(sino, im, txLUT, axLUT, subs, cnst, att, sync=True):
+    """Forward projection into `sino` (`[Nprj|68516, nsinos]` float32, overwritten), as
+    `petprj.fprj` (`prj_module.cu:232-425`, `prjf.cu:209-320`).  `att=1` gives
+    attenuation factors exp(-line integral)."""
+    dev = device_of(cnst)
+    nsn = nsinos_of(cnst)
+    g = get_geometry(txLUT, axLUT, dev)
+    d_subs, nprj = _subs_arg(subs, dev)
+    if tuple(np.shape(sino)) != (nprj, nsn):
+        raise ValueError(f'sino must have shape {(nprj, nsn)}, got {tuple(np.shape(sino))}')
+    if tuple(np.shape(im)) != IMG_SHAPE:
+        raise ValueError(f'image must have shape {IMG_SHAPE}')
+    d_im = to_device(im, np.float32, dev)
+    out = sino if (isinstance(sino, torch.Tensor) and sino.is_cuda and sino.is_contiguous()
+                   and sino.dtype == torch.float32) else torch.empty((nprj, nsn), device=dev)
+    _lib.check(_lib.load().nb_fprj(g.handle, dev_ptr(out), dev_ptr(d_im),
+                                   dev_ptr(d_subs) if d_subs is not None else None, nprj,
+                                   int(cnst['SPN']), int(att), stream_ptr(dev)))
+    if sync:
+        g.check()
+    _writeback(sino, out)
+
+
+def bprj(bimg, sino, txLUT, axLUT, subs, cnst, sync=True):
+    """Back projection into `bimg` (`[320,320,127]` float32, overwritten), as `petprj.bprj`
+    (`prj_module.cu:430-608`, `prjb.cu:190-308`)."""
+    dev = device_of(cnst)
+    nsn = nsinos_of(cnst)
+    g = get_geometry(txLUT, axLUT, dev)
+    d_subs, nprj = _subs_arg(subs, dev)
+    if tuple(np.shape(sino)) != (nprj, nsn):
+        raise ValueError(f'sino must have shape {(nprj, nsn)}, got {tuple(np.shape(sino))}')
+    if tuple(np.shape(bimg)) != IMG_SHAPE:
+        raise ValueError(f'image must have shape {IMG_SHAPE}')
+    d_sino = to_device(sino, np.float32, dev)
+    out = bimg if (isinstance(bimg, torch.Tensor) and bimg.is_cuda and bimg.is_contiguous()
+                   and bimg.dtype == torch.float32) else torch.empty(IMG_SHAPE, device=dev)
+    _lib.check(_lib.load().nb_bprj(g.handle, dev_ptr(out), dev_ptr(d_sino),
+                                   dev_ptr(d_subs) if d_subs is not None else None, nprj,
+                                   int(cnst['SPN']), stream_ptr(dev)))
+    if sync:
+        g.check()
+    _writeback(bimg, out)
+
+
+def to_col128(im: torch.Tensor, nimg: int = 1) -> torch.Tensor:
+    out = torch.empty((nimg, COL128), device=im.device, dtype=torch.float32)
+    _lib.check(_lib.load().nb_im_to_col128(dev_ptr(out), dev_ptr(im.contiguous()), nimg,
+                                           stream_ptr(im.device)))
+    return out
+
+
+def from_col128(im128: torch.Tensor, nimg: int = 1) -> torch.Tensor:
+    out = torch.empty((nimg,) + IMG_SHAPE, device=im128.device, dtype=torch.float32)
+    _lib.check(_lib.load().nb_col128_to_im(dev_ptr(out), dev_ptr(im128.contiguous()), nimg,
+                                           stream_ptr(im128.device)))
+    return out
+
+
+def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axLUT, cnst):
+    """One OSEM iteration over all subsets, updating `img` in place, as `petprj.osem`
+    (`prj_module.cu:613-839`, `recon.cu:318-521`).
+
+    `subs` is `[Nsub, 1+Nprj]` with `subs[i,0] = Nprj`; `sensimg` is `[Nsub,320,320,127]`;
+    `krnl[0,0] < 0` means no resolution modelling (the only mode provided)."""
+    dev = device_of(cnst)
+    if int(cnst['SPN']) != 11:
+        raise NotImplementedError('nipet_b200.petprj.osem runs span-11 data')
+    k = np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor) else krnl).reshape(-1)
+    if k.size and k[0] >= 0:
+        raise NotImplementedError('resolution modelling (PSF kernel) is not provided')
+    g = get_geometry(txLUT, axLUT, dev)
+    nsn = 837
+    lib = _lib.load()
+    st = stream_ptr(dev)
+    subs_np = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs)
+    nsub = subs_np.shape[0]
+    for a, nm in ((psng, 'psng'), (rsng, 'rsng'), (nsng, 'nsng'), (asng, 'asng')):
+        if tuple(np.shape(a)) != (NAW, nsn):
+            raise ValueError(f'{nm} must have shape {(NAW, nsn)}')
+    d_psng = to_device(psng, np.uint16, dev)
+    d_r = to_device(rsng, np.float32, dev)
+    d_s = to_device(ssng, np.float32, dev) if ssng is not None else None
+    d_n = to_device(nsng, np.float32, dev)
+    d_a = to_device(asng, np.float32, dev)
+    rs = torch.empty((NAW, nsn), device=dev, dtype=torch.float32)
+    _lib.check(lib.nb_osem_rs(dev_ptr(rs), dev_ptr(d_r), dev_ptr(d_s) if d_s is not None else None,
+                              dev_ptr(d_a), dev_ptr(d_n), NAW * nsn, st))
+    d_img = to_device(img, np.float32, dev)
+    img128 = to_col128(d_img)
+    sens = to_device(sensimg, np.float32, dev)
+    if tuple(sens.shape) != (nsub,) + IMG_SHAPE:
+        raise ValueError(f'sensimg must have shape {(nsub,) + IMG_SHAPE}')
+    sens128 = to_col128(sens, nsub)
+    m = to_device(msk, np.float32, dev)
+    msk128 = (to_col128(m) > 0.5).to(torch.uint8)
+    bimg128 = torch.empty_like(img128)
+    for i in range(nsub):
+        nprj = int(subs_np[i, 0])
+        d_sub = to_device(subs_np[i, 1:1 + nprj].astype(np.int32), np.int32, dev)
+        _lib.check(lib.nb_osem_subset(g.handle, dev_ptr(img128), dev_ptr(bimg128),
+                                      dev_ptr(sens128[i]), dev_ptr(msk128), dev_ptr(d_psng),
+                                      dev_ptr(rs), dev_ptr(d_sub), nprj, st))
+    out = from_col128(img128)
+    g.check()
+    _writeback(img, out[0])

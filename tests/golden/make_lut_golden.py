@@ -1,0 +1,62 @@
+"""Generate `lut_golden.npz` by running the reference's own Python LUT builders.
+
+The reference package cannot be imported here (it needs `cuvec`, `ninst`, `nimpa`
+and compiled CUDA modules), but its LUT builders are pure numpy.  This script
+extracts `axial_lut`, `transaxial_lut` (`niftypet/nipet/mmraux.py`) and
+`get_subsets14` (`niftypet/nipet/prj/mmrrec.py`) from the reference sources with
+`ast`, executes them unchanged, and stores their outputs as golden vectors.
+
+The scanner constants (`Cnt`) come from the un-vendored `ninst` package in the
+reference; the values used here are `nipet_b200.geometry.get_mmr_constants()`.
+
+Run from the repository root, in a container that has the reference checkout:
+    python tests/golden/make_lut_golden.py /root/reference
+"""
+import ast
+import logging
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from nipet_b200.geometry import get_mmr_constants  # noqa: E402
+
+
+def _extract(path, names):
+    src = open(path).read()
+    tree = ast.parse(src)
+    body = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in names]
+    mod = ast.Module(body=body, type_ignores=[])
+    ns = {'np': np, 'pi': math.pi, 'math': math, 'log': logging.getLogger('ref')}
+    exec(compile(mod, path, 'exec'), ns)
+    return ns
+
+
+def main(ref_root):
+    nipet = os.path.join(ref_root, 'niftypet', 'nipet')
+    aux = _extract(os.path.join(nipet, 'mmraux.py'), {'axial_lut', 'transaxial_lut'})
+    rec = _extract(os.path.join(nipet, 'prj', 'mmrrec.py'), {'get_subsets14'})
+    Cnt = get_mmr_constants()
+    tx = aux['transaxial_lut'](Cnt)
+    Cnt['Naw'] = tx['Naw']
+    ax = aux['axial_lut'](Cnt)
+    params = {'Cnt': Cnt, 'txLUT': tx, 'axLUT': ax}
+    subs = np.stack([rec['get_subsets14'](n, params)[0] for n in range(14)]).astype(np.int32)
+    out = {
+        'crs': tx['crs'], 's2cF': tx['s2cF'], 's2c': tx['s2c'], 'aw2ali': tx['aw2ali'],
+        'msino': tx['msino'], 'crsri': tx['crsri'], 'Naw': np.int64(tx['Naw']),
+        'li2rno': ax['li2rno'], 'li2sn': ax['li2sn'], 'li2sn1': ax['li2sn1'],
+        'li2nos': ax['li2nos'], 'li2rng': ax['li2rng'], 'sn1_rno': ax['sn1_rno'],
+        'sn1_ssrb': ax['sn1_ssrb'], 'sn1_sn11': ax['sn1_sn11'], 'sn11_ssrb': ax['sn11_ssrb'],
+        'subsets14': subs}
+    dst = os.path.join(HERE, 'lut_golden.npz')
+    np.savez_compressed(dst, **out)
+    print('wrote', dst, {k: getattr(v, 'shape', ()) for k, v in out.items()})
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
