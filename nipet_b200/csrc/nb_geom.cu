@@ -13,6 +13,7 @@
 
 #include "nb_axial.cuh"
 #include "nb_internal.cuh"
+#include "nb_project.cuh"
 
 // ---------------------------------------------------------------------------------------
 // One thread per LOR: tt[10] and the crossing sequence tv[1807] (reference layout).
@@ -185,6 +186,22 @@ __global__ void k_expand_steps(const float *__restrict__ tt, const unsigned char
   hdr[idx] = make_float4(t[5], t[7], t[6], __int_as_float(n));
 }
 
+// longest walk segment (tn - tp) of every LOR, as float bits (segments are >= 0)
+__global__ void k_maxseg(const float4 *__restrict__ hdr, const float *__restrict__ st, int naw,
+                         unsigned *out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= naw) return;
+  const float4 h = hdr[idx];
+  const int n = __float_as_int(h.w);
+  float tp = h.x, m = 0.f;
+  for (int k = 0; k < n; k++) {
+    const float tn = st[(size_t)idx * NB_STEP_STRIDE + k];
+    m = fmaxf(m, fabsf(__fsub_rn(tn, tp)));
+    tp = tn;
+  }
+  atomicMax(out, __float_as_uint(m));
+}
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -355,6 +372,37 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
     if (herr) {
       nb_set_error_msg("nb_geom_create: step expansion reported device error %d", herr);
       st = NB_ERR_DEVICE;
+      goto fail;
+    }
+    // Walk checks: every ray stays inside z in [0, 127) (the projector kernels index
+    // shared memory by it) and the longest segment sets the fixed-point headroom of the
+    // back projector (242 overlapping rays per column slot at most).
+    cudaMemset(g->d_err, 0, sizeof(int));
+    nbk::k_check_walk<<<naw, 256>>>(g->d_hdr, g->d_st, g->d_rays, naw, g->d_err);
+    unsigned *d_seg = (unsigned *)d_tv;  // reuse the table buffer
+    cudaMemset(d_seg, 0, sizeof(unsigned));
+    k_maxseg<<<(naw + 255) / 256, 256>>>(g->d_hdr, g->d_st, naw, d_seg);
+    unsigned segbits = 0;
+    int nbad = 0;
+    cudaError_t e = cudaMemcpy(&nbad, g->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&segbits, d_seg, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      st = nb_cuda_fail(e, "nb_geom_create walk check", __FILE__, __LINE__);
+      goto fail;
+    }
+    cudaMemset(g->d_err, 0, sizeof(int));
+    if (nbad) {
+      nb_set_error_msg("nb_geom_create: %d ray positions leave the axial FOV", nbad);
+      st = NB_ERR_DATA;
+      goto fail;
+    }
+    memcpy(&g->maxseg, &segbits, sizeof(float));
+    double bound = 242.0 * (g->maxseg > 0.f ? g->maxseg : 1.0);
+    int lb = (int)ceil(log2(bound));
+    g->fxbits = 31 - lb;
+    if (g->fxbits < 16) {
+      nb_set_error_msg("nb_geom_create: walk segments too long (%g cm)", (double)g->maxseg);
+      st = NB_ERR_DATA;
       goto fail;
     }
   }

@@ -34,6 +34,8 @@ struct nb_geom {
   int16_t *d_bin11;  // [837][8] rays summed into each span-11 sinogram (-1 padded)
   int16_t *d_bin1;   // [4084] ray of each span-1 sinogram
   float *d_scratch128;   // one col128 image (reference-layout entry points)
+  float maxseg;          // longest walk segment of the geometry (cm)
+  int fxbits;            // fixed-point headroom of the backward accumulators
   int *d_err;            // device error flag
   // host copies of the LUTs (for nb_geom_tables)
   float h_crs[504 * 4];

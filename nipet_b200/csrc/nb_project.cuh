@@ -1,0 +1,455 @@
+// nb_project.cuh -- the persistent Siddon projector kernel (forward, backward and the
+// fused OSEM sub-iteration), used by nb_prj.cu.
+//
+// Reference semantics: prj/src/prjf.cu:33-206 (fprj_drct, fprj_oblq), prj/src/prjb.cu:33-187
+// (bprj_drct, bprj_oblq), prj/src/recon.cu:252-309 and :459-497 (OSEM sub-iteration).
+//
+// B200 design
+//  * Persistent grid, one 1024-thread CTA per SM.  A CTA owns one LOR (a transaxial
+//    sinogram bin) at a time and computes all 4084 rays (span-1 ring pairs) of it;
+//    thread t handles rays t, t+1024, t+2048, t+3072 of the canonical ray order.
+//  * The LOR's voxel columns (512 B each in the col128 layout) are streamed into shared
+//    memory in chunks of CH columns with TMA bulk copies (cp.async.bulk + mbarrier),
+//    double buffered, so every voxel read of the walk is a shared-memory load.
+//  * Span-11 sinograms are formed by a deterministic in-CTA sum over the span-1 rays
+//    (no global atomics, run-to-run identical); each CTA writes whole sinogram rows.
+//  * Back projection accumulates the LOR's columns in shared memory as int32 fixed point
+//    (native shared integer atomics; the scale is a power of two chosen per LOR so no
+//    column slot can overflow), converts each finished chunk to float in a staging
+//    buffer and flushes it with one TMA bulk reduce-add per column
+//    (cp.reduce.async.bulk .add.f32) instead of one global atomic per voxel visit.
+//  * The OSEM kernel fuses, per LOR: forward projection, the ratio
+//    y / (Ax + (r+s)/(an)) and the back projection of the ratio -- the subset
+//    sinogram never goes to HBM.
+//
+// The axial voxel index of every ray is kept in the de-interleaved column slot `zi`
+// (even z in [0,64), odd z in [64,127)); a crossing moves it by `dz`, which alternates
+// between two values (+64/-63 upwards, +63/-64 downwards).  nb_geom_create verifies
+// once that no ray of the geometry leaves z in [0, 127], so the walk needs no clamp.
+#pragma once
+#include "nb_axial.cuh"
+#include "nb_internal.cuh"
+
+namespace nbk {
+
+constexpr int NT = 1024;  // threads per CTA
+constexpr int RPT = 4;    // rays per thread (NT * RPT >= 4084)
+constexpr uint32_t WAIT_POLLS = 1u << 20;
+
+enum { MODE_FWD = 0, MODE_BWD = 1, MODE_OSEM = 2 };
+
+struct PrjArgs {
+  const int32_t *scol;
+  const float *st;
+  const float4 *hdr;
+  const nb_ray *rays;
+  const int16_t *bin11;
+  const int16_t *bin1;
+  const int32_t *subs;
+  int nprj;
+  int naw;
+  int span;              // 1 or 11
+  int att;               // forward: 0 emission, 1 attenuation
+  const float *img;      // col128 image read by forward passes
+  float *bimg;           // col128 image accumulated by backward passes
+  float *sino;           // forward output [nprj][nout]
+  const float *sino_in;  // backward input [nprj][nout]
+  const uint16_t *psng;  // OSEM prompts [naw][nout]
+  const float *rs;       // OSEM (r+s)/(an) [naw][nout]
+  int fxbits;            // backward fixed point: |value| * 2^fxbits / 2^e fits every slot
+  int *err;
+};
+
+template <int MODE, int CH> struct Smem {
+  static constexpr bool HAS_I = MODE != MODE_FWD;
+  static constexpr size_t buf_bytes = 2ull * CH * NB_COLW * sizeof(float);
+  static constexpr size_t fbuf_off = 0;                 // forward columns / backward staging
+  static constexpr size_t ibuf_off = fbuf_off + buf_bytes;  // backward int32 accumulators
+  static constexpr size_t tn_off = ibuf_off + (HAS_I ? buf_bytes : 0);
+  static constexpr size_t vals_off = tn_off + 2ull * CH * sizeof(float);
+  static constexpr size_t rat_off = vals_off + 4096 * sizeof(float);
+  static constexpr size_t misc_off = rat_off + (MODE == MODE_OSEM ? 4096 * sizeof(float) : 0);
+  static constexpr size_t total = misc_off + 64;
+};
+
+struct Job {
+  int p;    // sinogram row
+  int lor;  // LOR index (subs[p])
+  int n;    // steps of the LOR
+  int nch;  // chunks per pass
+  int c;    // chunk index in the LOR's job list (OSEM: [0,nch) forward, [nch,2nch) backward)
+  int valid;
+};
+
+template <int CH>
+__device__ __forceinline__ void job_load(const PrjArgs &a, int p, Job &J) {
+  J.p = p;
+  J.valid = p < a.nprj;
+  J.c = 0;
+  if (!J.valid) return;
+  const int lor = a.subs ? a.subs[p] : p;
+  if (lor < 0 || lor >= a.naw) {
+    if (threadIdx.x == 0) nb_set_error(a.err, NB_DEVERR_BAD_LOR);
+    J.lor = 0;
+    J.n = 0;
+  } else {
+    J.lor = lor;
+    J.n = __float_as_int(a.hdr[lor].w);
+  }
+  J.nch = J.n > 0 ? (J.n + CH - 1) / CH : 1;
+}
+
+template <int MODE, int CH> __device__ __forceinline__ void job_next(const PrjArgs &a, Job &J) {
+  const int per_lor = (MODE == MODE_OSEM) ? 2 * J.nch : J.nch;
+  if (++J.c >= per_lor) job_load<CH>(a, J.p + gridDim.x, J);
+}
+
+template <int MODE> __device__ __forceinline__ bool job_is_load(const Job &J) {
+  if (MODE == MODE_FWD) return true;
+  if (MODE == MODE_BWD) return false;
+  return J.c < J.nch;
+}
+
+template <int MODE> __device__ __forceinline__ int job_chunk(const Job &J) {
+  return (MODE == MODE_OSEM && J.c >= J.nch) ? J.c - J.nch : J.c;
+}
+
+// warp 0: TMA loads of one forward chunk (its columns + exit parameters)
+template <int CH>
+__device__ __forceinline__ void issue_load(const PrjArgs &a, const Job &J, int chunk,
+                                           float *cols, float *tnb, uint64_t *bar) {
+  const int lane = threadIdx.x & 31;
+  const int s0 = chunk * CH;
+  const int n = max(0, min(CH, J.n - s0));
+  const uint32_t tn_bytes = max(16u, (uint32_t)((n * 4 + 15) & ~15));
+  if (lane == 0) nb_mbar_arrive_expect_tx(bar, (uint32_t)n * (NB_COLW * 4) + tn_bytes);
+  __syncwarp();
+  const int32_t *sc = a.scol + (size_t)J.lor * NB_STEP_STRIDE + s0;
+  for (int i = lane; i < n; i += 32)
+    nb_bulk_g2s(cols + (size_t)i * NB_COLW, a.img + (size_t)sc[i] * NB_COLW, NB_COLW * 4, bar);
+  if (lane == 0) nb_bulk_g2s(tnb, a.st + (size_t)J.lor * NB_STEP_STRIDE + s0, tn_bytes, bar);
+}
+
+// warp 0: exit parameters of one backward chunk (plain loads; read after a CTA barrier)
+template <int CH>
+__device__ __forceinline__ void load_tn(const PrjArgs &a, const Job &J, int chunk, float *tnb) {
+  const int lane = threadIdx.x & 31;
+  const int s0 = chunk * CH;
+  const int n = max(0, min(CH, J.n - s0));
+  for (int i = lane; i < n; i += 32) tnb[i] = a.st[(size_t)J.lor * NB_STEP_STRIDE + s0 + i];
+}
+
+struct RayState {
+  float acc[RPT];  // forward: line integral; backward: value to spread (bin * s * scale)
+  float tzc[RPT];  // next axial crossing
+  float dtz[RPT];
+  int zi[RPT];     // column slot of the current voxel
+  int dz[RPT];     // slot change at the next crossing
+  int dir[RPT];    // +1 / -1 (0: direct plane)
+  float tp;
+};
+
+__device__ __forceinline__ void rays_init(const PrjArgs &a, const float4 h, RayState &S) {
+  S.tp = h.x;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    const int ray = threadIdx.x + NT * r;
+    S.acc[r] = 0.f;
+    if (ray < NB_NRAYS) {
+      nb_axial A;
+      nb_axial_setup(a.rays[ray], h.y, h.x, h.z, A);
+      S.zi[r] = nb_zi(A.w);
+      S.tzc[r] = A.tzc;
+      S.dtz[r] = A.dtz;
+      S.dir[r] = A.dir;
+      // slot change of the first crossing: parity of w decides (+64/-63 up, +63/-64 down)
+      S.dz[r] = A.dir > 0 ? ((A.w & 1) ? -63 : 64) : (A.dir < 0 ? ((A.w & 1) ? -64 : 63) : 0);
+    } else {
+      S.zi[r] = 127;  // padding slot, never crosses
+      S.tzc[r] = __int_as_float(0x7f800000);
+      S.dtz[r] = 0.f;
+      S.dir[r] = 0;
+      S.dz[r] = 0;
+    }
+  }
+}
+
+// oblique length factor of ray r of this thread for a LOR of length atn
+__device__ __forceinline__ float ray_s(const PrjArgs &a, int ray, float atn) {
+  const nb_ray R = a.rays[ray];
+  if (R.kind == 0) return 1.f;
+  const float az_atn = __fdiv_rn(__fsub_rn(R.r1z, R.r0z), atn);
+  return __fsqrt_rn(__fmaf_rn(az_atn, az_atn, 1.0f));
+}
+
+// Forward walk over n steps of one chunk (prjf.cu:76-86 / :164-190).  The segment of a
+// step is [tp, min(tn, tzc)] in the current voxel and, at a crossing, [tzc, tn] in the
+// next one; a ray crosses at most one z plane per step, as in the reference.
+__device__ __forceinline__ void walk_fwd(RayState &S, const float *col0, const float *tnb, int n) {
+  float tp = S.tp;
+  for (int i = 0; i < n; ++i) {
+    const float tn = tnb[i];
+    const float *col = col0 + i * NB_COLW;
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      const float tz = S.tzc[r];
+      const float v0 = col[S.zi[r]];
+      const float fa = __fsub_rn(fminf(tn, tz), tp);
+      S.acc[r] = fmaf(fa, v0, S.acc[r]);
+      if (tn > tz) {
+        S.zi[r] += S.dz[r];
+        S.dz[r] = S.dir[r] - S.dz[r];
+        S.acc[r] = fmaf(__fsub_rn(tn, tz), col[S.zi[r]], S.acc[r]);
+        S.tzc[r] = __fadd_rn(tz, S.dtz[r]);
+      }
+    }
+    tp = tn;
+  }
+  S.tp = tp;
+}
+
+// Backward walk (prjb.cu:70-77 / :153-178): the same segments, spread as int32 fixed point.
+__device__ __forceinline__ void walk_bwd(RayState &S, int *col0, const float *tnb, int n) {
+  float tp = S.tp;
+  for (int i = 0; i < n; ++i) {
+    const float tn = tnb[i];
+    int *col = col0 + i * NB_COLW;
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      const float tz = S.tzc[r];
+      const float fa = __fsub_rn(fminf(tn, tz), tp);
+      atomicAdd(col + S.zi[r], __float2int_rn(fa * S.acc[r]));
+      if (tn > tz) {
+        S.zi[r] += S.dz[r];
+        S.dz[r] = S.dir[r] - S.dz[r];
+        atomicAdd(col + S.zi[r], __float2int_rn(__fsub_rn(tn, tz) * S.acc[r]));
+        S.tzc[r] = __fadd_rn(tz, S.dtz[r]);
+      }
+    }
+    tp = tn;
+  }
+  S.tp = tp;
+}
+
+template <int MODE, int CH>
+__global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  using L = Smem<MODE, CH>;
+  float *fbuf = reinterpret_cast<float *>(smem_raw + L::fbuf_off);
+  int *ibuf = reinterpret_cast<int *>(smem_raw + L::ibuf_off);
+  float *tnbuf = reinterpret_cast<float *>(smem_raw + L::tn_off);
+  float *vals = reinterpret_cast<float *>(smem_raw + L::vals_off);
+  float *rat = reinterpret_cast<float *>(smem_raw + L::rat_off);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + L::misc_off);
+  int *sflag = reinterpret_cast<int *>(smem_raw + L::misc_off + 16);
+  unsigned *smax = reinterpret_cast<unsigned *>(smem_raw + L::misc_off + 24);  // [2]
+
+  const int tid = threadIdx.x;
+  const bool warp0 = tid < 32;
+  const int nout = a.span == 11 ? NB_NSN11 : NB_NSN1;
+
+  if (tid == 0) {
+    nb_mbar_init(&bars[0], 1);
+    nb_mbar_init(&bars[1], 1);
+    *sflag = 0;
+    smax[0] = 0u;
+    smax[1] = 0u;
+    nb_fence_mbar_init();
+  }
+  if (L::HAS_I)
+    for (int i = tid; i < 2 * CH * NB_COLW; i += NT) ibuf[i] = 0;
+  __syncthreads();
+
+  Job J, P;  // consumer cursor (all threads), producer cursor (warp 0)
+  job_load<CH>(a, blockIdx.x, J);
+  if (warp0) {
+    P = J;
+    for (int k = 0; k < 2 && P.valid; k++) {
+      if (job_is_load<MODE>(P))
+        issue_load<CH>(a, P, job_chunk<MODE>(P), fbuf + (size_t)k * CH * NB_COLW, tnbuf + k * CH,
+                       &bars[k]);
+      else
+        load_tn<CH>(a, P, job_chunk<MODE>(P), tnbuf + k * CH);
+      job_next<MODE, CH>(a, P);
+    }
+  }
+  __syncthreads();
+
+  RayState S;
+  float inv_scale = 0.f;
+  uint32_t phase = 0;  // bit b: parity of the next completion of bars[b]
+  int j = 0, nlor = 0;
+  while (J.valid) {
+    const int b = j & 1;
+    float *fb = fbuf + (size_t)b * CH * NB_COLW;
+    int *ib = ibuf + (size_t)b * CH * NB_COLW;
+    float *tb = tnbuf + b * CH;
+    const bool load = job_is_load<MODE>(J);
+    const int chunk = job_chunk<MODE>(J);
+    const int n = max(0, min(CH, J.n - chunk * CH));
+    const float4 h = a.hdr[J.lor];
+
+    if (chunk == 0) {
+      rays_init(a, h, S);
+      if (!load) {
+        // values to spread and the per-LOR fixed-point scale: a power of two such that
+        // the largest slot sum (<= 242 rays x the longest segment x max|value|) stays
+        // below 2^31 (fxbits is derived from the geometry's longest segment)
+        float m = 0.f;
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+          const int ray = tid + NT * r;
+          float v = 0.f;
+          if (ray < NB_NRAYS) {
+            const nb_ray R = a.rays[ray];
+            const int o = a.span == 11 ? R.out11 : R.out1;
+            const float bin = (MODE == MODE_BWD) ? a.sino_in[(size_t)J.p * nout + o] : rat[o];
+            v = bin * ray_s(a, ray, h.y);
+          }
+          S.acc[r] = v;
+          m = fmaxf(m, fabsf(v));
+        }
+        for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const int par = nlor & 1;
+        if ((tid & 31) == 0 && m > 0.f) atomicMax(&smax[par], __float_as_uint(m));
+        __syncthreads();
+        const unsigned mb = smax[par];
+        if (tid == 0) smax[par ^ 1] = 0u;
+        float scale = 0.f;
+        inv_scale = 0.f;
+        if (mb != 0u && (mb >> 23) < 255u) {
+          const int e = (int)(mb >> 23) - 126;  // max < 2^e
+          scale = ldexpf(1.f, a.fxbits - e);
+          inv_scale = ldexpf(1.f, e - a.fxbits);
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++) S.acc[r] *= scale;
+        ++nlor;
+      }
+    }
+
+    if (load) {
+      if (!nb_mbar_wait(&bars[b], (phase >> b) & 1u, WAIT_POLLS)) atomicExch(sflag, 1);
+      phase ^= 1u << b;
+      walk_fwd(S, fb, tb, n);
+    } else {
+      // the bulk reduce that last read staging buffer b must be done before we refill it
+      if (warp0) nb_bulk_wait_read<1>();
+      walk_bwd(S, ib, tb, n);
+      __syncthreads();
+      // int32 accumulators -> float staging (and back to zero for their next use)
+      const int nv = n * NB_COLW / 4;
+      int4 *i4 = reinterpret_cast<int4 *>(ib);
+      float4 *f4 = reinterpret_cast<float4 *>(fb);
+      for (int x = tid; x < nv; x += NT) {
+        const int4 q = i4[x];
+        // slot 127 (the padding slice) is never written back
+        const float w4 = (x & 31) == 31 ? 0.f : (float)q.w * inv_scale;
+        f4[x] = make_float4((float)q.x * inv_scale, (float)q.y * inv_scale,
+                            (float)q.z * inv_scale, w4);
+        i4[x] = make_int4(0, 0, 0, 0);
+      }
+      nb_fence_proxy_async_smem();
+    }
+
+    // forward epilogue at the end of the LOR's forward pass
+    if (load && chunk == J.nch - 1) {
+#pragma unroll
+      for (int r = 0; r < RPT; r++) {
+        const int ray = tid + NT * r;
+        if (ray < NB_NRAYS) {
+          float v = S.acc[r] * ray_s(a, ray, h.y);
+          if (MODE == MODE_FWD && a.att == 1) {
+            v = expf(-v);
+            if (a.span == 11) v = v / (float)a.rays[ray].nos;
+          }
+          vals[ray] = v;
+        }
+      }
+      __syncthreads();
+      for (int o = tid; o < nout; o += NT) {
+        float v;
+        if (a.span == 11) {
+          v = 0.f;
+          const int16_t *lst = a.bin11 + o * 8;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int ray = lst[q];
+            if (ray >= 0) v += vals[ray];
+          }
+        } else {
+          v = vals[a.bin1[o]];
+        }
+        if (MODE == MODE_FWD) {
+          a.sino[(size_t)J.p * nout + o] = v;
+        } else {
+          const size_t g = (size_t)J.lor * nout + o;
+          const float e = v + a.rs[g];
+          const float y = (float)a.psng[g];
+          rat[o] = (e > -0.000001f && e < 0.000001f) ? 0.f : __fdiv_rn(y, e);
+        }
+      }
+    }
+
+    __syncthreads();  // buffer b, the staging data and rat are complete / free
+    if (*sflag) break;
+
+    if (warp0) {
+      if (MODE != MODE_FWD) {
+        if (!load) {
+          const int32_t *sc = a.scol + (size_t)J.lor * NB_STEP_STRIDE + chunk * CH;
+          for (int i = tid; i < n; i += 32)
+            nb_bulk_reduce_add_f32(a.bimg + (size_t)sc[i] * NB_COLW, fb + (size_t)i * NB_COLW,
+                                   NB_COLW * 4);
+        }
+        nb_bulk_commit();  // one group per job and lane (empty for forward jobs)
+      }
+      // producer: job j+2 reuses buffer b
+      if (P.valid) {
+        if (job_is_load<MODE>(P)) {
+          if (MODE == MODE_OSEM) nb_bulk_wait_read<0>();
+          issue_load<CH>(a, P, job_chunk<MODE>(P), fb, tb, &bars[b]);
+        } else {
+          load_tn<CH>(a, P, job_chunk<MODE>(P), tb);
+        }
+        job_next<MODE, CH>(a, P);
+      }
+    }
+    job_next<MODE, CH>(a, J);
+    ++j;
+  }
+  if (*sflag && tid == 0) nb_set_error(a.err, NB_DEVERR_MBAR_TIMEOUT);
+  if (warp0 && MODE != MODE_FWD) nb_bulk_wait_all<0>();
+}
+
+// Verifies that every ray of every LOR keeps its axial voxel in [0, 127]: the walk
+// kernels index shared memory by it without clamping.  z = 127 is one slice above the
+// image; it maps to the column's zero padding slot (reads 0, back projections into it
+// are discarded).  In the mMR geometry exactly one ray step reaches it (the last step of
+// rings 59->63 on LOR 24839).  One block per LOR.
+static __global__ void k_check_walk(const float4 *__restrict__ hdr, const float *__restrict__ st,
+                             const nb_ray *__restrict__ rays, int naw, int *bad) {
+  const int lor = blockIdx.x;
+  if (lor >= naw) return;
+  const float4 h = hdr[lor];
+  const int n = __float_as_int(h.w);
+  int nbad = 0;
+  for (int ray = threadIdx.x; ray < NB_NRAYS; ray += blockDim.x) {
+    nb_axial A;
+    nb_axial_setup(rays[ray], h.y, h.x, h.z, A);
+    int w = A.w;
+    float tzc = A.tzc;
+    if (w < 0 || w > NB_IMZ) nbad++;
+    for (int k = 0; k < n; k++) {
+      const float tn = st[(size_t)lor * NB_STEP_STRIDE + k];
+      if (tn > tzc) {
+        w += A.dir;
+        tzc = __fadd_rn(tzc, A.dtz);
+        if (w < 0 || w > NB_IMZ) nbad++;
+      }
+    }
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+}  // namespace nbk

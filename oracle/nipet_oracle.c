@@ -500,6 +500,49 @@ long long orc_count_reads(const float *tt, const unsigned char *tv, const float 
   return tot;
 }
 
+/* Every (LOR, ring pair, sign, step) at which a ray's axial voxel leaves [0, 127):
+ * writes up to `cap` records (lor, li, sign(+1/-1/0 direct), step, w); returns the count. */
+int orc_scan_oob(const float *tt, const unsigned char *tv, const float *li2rng, int naw,
+                 int *rec, int cap) {
+  int cnt = 0;
+  int *uvs = malloc(sizeof(int) * STEP_CAP);
+  float *tps = malloc(sizeof(float) * STEP_CAP), *tns = malloc(sizeof(float) * STEP_CAP);
+  for (int p = 0; p < naw; p++) {
+    int n = expand_lor(tt, tv, p, uvs, tps, tns, STEP_CAP);
+    const float *t = tt + (size_t)N_TT * p;
+    for (int ixz = NRINGS; ixz < NLI2R; ixz++) {
+      axial_t A;
+      axial_setup(li2rng, ixz, t[7], t[5], t[6], &A);
+      int w = A.w, w_ = A.w_;
+      float tzc = A.tzc;
+      for (int k = -1; k < n; k++) {
+        if (k >= 0 && (tns[k] - tzc) > 0) {
+          w += A.sgnaz;
+          w_ -= A.sgnaz;
+          tzc += A.dtz;
+        }
+        int ws[2] = {w, w_};
+        for (int q = 0; q < 2; q++)
+          if (ws[q] < 0 || ws[q] >= SZ_IMZ) {
+            if (cnt < cap) {
+              int *r = rec + 5 * cnt;
+              r[0] = p;
+              r[1] = ixz;
+              r[2] = q ? -1 : 1;
+              r[3] = k;
+              r[4] = ws[q];
+            }
+            cnt++;
+          }
+      }
+    }
+  }
+  free(uvs);
+  free(tps);
+  free(tns);
+  return cnt;
+}
+
 /* Step count of every LOR (prjf.cu loop trip count, tt[9]-3). */
 void orc_step_counts(const float *tt, int naw, int *nsteps) {
   for (int i = 0; i < naw; i++) nsteps[i] = (int)tt[(size_t)N_TT * i + 9] - 3;
