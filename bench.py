@@ -1,0 +1,433 @@
+"""Benchmark of the mMR reconstruction hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload osem|hist]
+
+Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand in for):
+  osem  one full OSEM reconstruction per step: 14 sensitivity images + 4 iterations x 14
+        subsets, span-11 (837 x 252 x 344 sinograms), 320x320x127 float32 image, prompts
+        from a brain phantom with water attenuation, log-normal crystal efficiencies and
+        20% uniform randoms at 3e7 counts.  Metric: reconstructions per second.
+  hist  list-mode histogramming of a synthetic 32-bit mMR event stream (events/s).
+
+`value` is measured on device-resident inputs (CUDA events, barrier + synchronize on
+both sides, L2 flushed between steps); `e2e` times the public drop-in API
+(`petprj.bprj` / `petprj.osem` with host numpy arrays, host<->device copies inside the
+timed region).  Under torchrun (N > 1) every rank reconstructs its own scan (replicas,
+weak scaling) and the slowest rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NAW, NSN11 = 68516, 837
+METRIC = {'osem': ('OSEM recon/s span-11 320x320x127', 'recon/s'),
+          'hist': ('list-mode histogram events/s', 'events/s')}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def _traffic(name):
+    try:
+        with open(os.path.join(ROOT, 'profiles', 'traffic.json')) as f:
+            return json.load(f).get(name)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', f'--id={index}', f'--query-gpu={q}',
+                                       '--format=csv,noheader,nounits', '-lms', '200'],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {'sm_mhz': statistics.median(load), 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def _dist():
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if ws > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device('cuda', local))
+    return ws, rank, local
+
+
+def _max_over_ranks(x, ws, dev):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws, dev):
+    import torch
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[dev.index])
+    torch.cuda.synchronize(dev)
+
+
+# ---------------------------------------------------------------------------------------
+# CPU baselines: the FP64 oracle (NIPET has no CPU path), on a bounded sample
+# ---------------------------------------------------------------------------------------
+def cpu_osem_sample(params, seconds=12.0):
+    """Time OSEM sub-iterations (forward, ratio, back projection, update) of the oracle on
+    a growing number of LORs of subset 0 and extrapolate to one full reconstruction
+    (14 sensitivity back projections + 4 x 14 sub-iterations over 68516 LORs each)."""
+    from oracle import oracle as O
+    from nipet_b200 import geometry as G
+    O.set_threads(os.cpu_count() or 1)
+    orc = O.Oracle(params)
+    sub0 = G.get_subsets14(0, params)[0]
+    rng = np.random.default_rng(0)
+    x = np.ones((320, 320, 127), np.float32)
+    n = 64
+    while True:
+        lors = np.sort(rng.choice(sub0, size=min(n, sub0.size), replace=False)).astype(np.int32)
+        sino = rng.random((lors.size, NSN11)).astype(np.float32)
+        t = time.perf_counter()
+        e = orc.fprj(x, lors)
+        _ = sino / np.maximum(e, 1e-6)
+        orc.bprj(sino, lors)
+        dt = time.perf_counter() - t
+        if dt * 4 > seconds or n >= sub0.size:
+            break
+        n *= 2
+    per_lor = dt / lors.size
+    t_recon = per_lor * NAW * 4 + 0.5 * per_lor * NAW
+    return {'value': 1.0 / t_recon, 'unit': 'recon/s', 'cores': O.num_threads(),
+            'kind': 'port',
+            'sample': f'FP64 oracle, {lors.size} LORs of subset 0: forward+ratio+back '
+                      f'({dt:.2f} s), extrapolated to 4x14 sub-iterations + sensitivity '
+                      f'over 68516 LORs'}
+
+
+def cpu_hist_sample(lm, params, seconds=10.0):
+    from oracle import oracle as O
+    n = min(lm.size, 2_000_000)
+    t = time.perf_counter()
+    O.hist(lm[:n], params, span=11)
+    dt = time.perf_counter() - t
+    return {'value': n / dt, 'unit': 'events/s', 'cores': 1, 'kind': 'port',
+            'sample': f'oracle histogram of the first {n} words (single thread)'}
+
+
+# ---------------------------------------------------------------------------------------
+# OSEM workload
+# ---------------------------------------------------------------------------------------
+def run_osem(args, ws, rank, dev):
+    import torch
+    from nipet_b200 import _lib, geometry, mmrrec, petprj
+    from nipet_b200.device import dev_ptr, stream_ptr
+
+    params = geometry.get_mmrparams()
+    Cnt = dict(params['Cnt'], DEVID=dev.index)
+    scan = mmrrec.synthetic_scan(params, dev, seed=rank)
+    rec = mmrrec.Recon(params, scan['psng'], scan['rsng'], scan['nsng'], scan['asng'],
+                       ssng=scan['ssng'], device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=dev)
+
+    # per-launch algorithmic bytes of the fused OSEM kernel: 4 B per forward voxel read,
+    # 4 B per back-projection voxel update, plus the subset's prompt/(r+s)/(an) rows
+    _, per_lor = rec.geom.count_reads(per_lor=True)
+    v_sub = [int(per_lor[s.cpu().numpy()].sum()) for s in rec.subs]
+    bytes_sub = [8 * v + rec.nprj * NSN11 * (2 + 4) for v in v_sub]
+
+    lib = _lib.load()
+    st = stream_ptr(dev)
+    ev = []  # (start, stop) events around every fused sub-iteration call
+
+    def step(record):
+        rec.sensitivity()
+        img = rec.init_image()
+        for _ in range(4):
+            for i in range(rec.nsub):
+                if record:
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                rec.subiteration(img, i, st)
+                if record:
+                    e1.record()
+                    ev.append((e0, e1, i))
+        return img
+
+    for _ in range(args.warmup):
+        step(False)
+        flush.fill_(1.0)
+    rec.geom.check()
+    rec.launches = 0
+    clk = Clocks(dev.index) if rank == 0 else None
+    times = []
+    for k in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        img = step(True)
+        t1.record()
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+        flush.fill_(float(k))
+    clocks = clk.stop() if clk else None
+    rec.geom.check()
+    launches_per_step = rec.launches // args.steps
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    value = ws / t_step
+    # roofline of the dominant kernel (fused OSEM sub-iteration)
+    dur = [e0.elapsed_time(e1) / 1e3 for e0, e1, _ in ev]
+    byt = [bytes_sub[i] for _, _, i in ev]
+    achieved = sum(byt) / sum(dur) / 1e9
+    peak, peak_kind = _peaks()
+    tr = _traffic('osem_subiteration')
+
+    # e2e through the public drop-in API with host arrays (reference call pattern)
+    e2e = None
+    if args.e2e_steps > 0:
+        host = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
+        an = host['asng'] * host['nsng']
+        tab = mmrrec.subset_table(params)
+        msk = geometry.get_cylinder(Cnt, rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
+        krnl = np.full((3, 17), -1, np.float32)
+        sens = np.zeros((14, 320, 320, 127), np.float32)
+
+        def e2e_step():
+            for n in range(14):
+                rows = tab[n, 1:]
+                petprj.bprj(sens[n], an[rows], params['txLUT'], params['axLUT'], rows, Cnt)
+            img = np.ones((320, 320, 127), np.float32)
+            for _ in range(4):
+                petprj.osem(img, host['psng'], host['rsng'], host['ssng'], host['nsng'],
+                            host['asng'], tab, sens, msk, krnl, params['txLUT'],
+                            params['axLUT'], Cnt)
+            return img
+        e2e_step()
+        et = []
+        for _ in range(args.e2e_steps):
+            _barrier(ws, dev)
+            t = time.perf_counter()
+            e2e_step()
+            torch.cuda.synchronize(dev)
+            et.append(time.perf_counter() - t)
+        te = _max_over_ranks(float(np.mean(et)), ws, dev)
+        per_call_in = (host['psng'].nbytes + 4 * host['rsng'].nbytes + sens.nbytes
+                       + msk.size * 1 + 320 * 320 * 127 * 4 + tab.nbytes)
+        h2d = 14 * (an[tab[0, 1:]].nbytes + tab[0, 1:].nbytes) + 4 * per_call_in
+        d2h = 14 * 320 * 320 * 127 * 4 + 4 * 320 * 320 * 127 * 4
+        e2e = {'value': ws / te, 'unit': 'recon/s', 'h2d_bytes_per_step': int(h2d),
+               'd2h_bytes_per_step': int(d2h),
+               'path': 'petprj.bprj x14 + petprj.osem x4 with host numpy arrays'}
+
+    res = {
+        'ms_per_step': t_step * 1e3, 'value': value, 'e2e': e2e, 'clocks': clocks,
+        'gpu_launches': launches_per_step,
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak, 'traffic': tr,
+                     'kernel': 'k_project<OSEM> fused sub-iteration (nb_osem_subset)',
+                     'peak_kind': peak_kind,
+                     'bytes_per_launch_avg': float(np.mean(byt)),
+                     'launch_ms_avg': float(np.mean(dur)) * 1e3},
+        'config': {'workload': 'plain OSEM, span-11 837x252x344, 320x320x127 f32, '
+                               '4 it x 14 subsets + sensitivity, 3e7 counts',
+                   'global_batch': ws, 'parallelism': f'replicas x{ws}',
+                   'l2': 'flushed between steps (256 MB write)'},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        res['cpu_baseline'] = cpu_osem_sample(params)
+    return res
+
+
+# ---------------------------------------------------------------------------------------
+# list-mode histogram workload
+# ---------------------------------------------------------------------------------------
+def run_hist(args, ws, rank, dev):
+    import torch
+    from nipet_b200 import geometry, mmr_lmproc, phantoms
+    params = geometry.get_mmrparams()
+    Cnt = dict(params['Cnt'], SPN=11, BTP=0, DEVID=dev.index)
+    lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=rank,
+                                 device=dev)
+    lm_host = lm.cpu().numpy()
+    pl = mmr_lmproc.plan(lm_host)
+    for _ in range(args.warmup):
+        mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], Cnt, pl=pl, unpack=False)
+    torch.cuda.synchronize(dev)
+    times = []
+    clk = Clocks(dev.index) if rank == 0 else None
+    for _ in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], Cnt, pl=pl, unpack=True)
+        t1.record()
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+    clocks = clk.stop() if clk else None
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    nev = int(lm.numel())
+    # e2e: host words -> plan -> device -> histogram -> host sinograms
+    et = []
+    for _ in range(max(1, args.e2e_steps)):
+        t = time.perf_counter()
+        p2 = mmr_lmproc.plan(lm_host)
+        r = mmr_lmproc.hist_stream(lm_host, params['txLUT'], params['axLUT'], Cnt, pl=p2)
+        r['psn'].cpu()
+        r['dsn'].cpu()
+        torch.cuda.synchronize(dev)
+        et.append(time.perf_counter() - t)
+    te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    res = {'ms_per_step': t_step * 1e3, 'value': ws * nev / t_step,
+           'e2e': {'value': ws * nev / te, 'unit': 'events/s', 'h2d_bytes_per_step': nev * 4,
+                   'd2h_bytes_per_step': 2 * 2 * 72557856},
+           'clocks': clocks, 'gpu_launches': 3,
+           'roofline': None,
+           'config': {'workload': f'list-mode histogram span-11, {nev} words over '
+                                  f'{args.duration} s', 'global_batch': ws,
+                      'parallelism': f'replicas x{ws}', 'l2': 'input larger than L2'}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        res['cpu_baseline'] = cpu_hist_sample(lm_host, params)
+    return res
+
+
+# ---------------------------------------------------------------------------------------
+# reference arm: NIPET has no CPU path; its algorithm restated as the FP64 oracle on the
+# host cores (bounded samples of the same workload)
+# ---------------------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return None
+    from nipet_b200 import geometry
+    params = geometry.get_mmrparams()
+    metric, unit = METRIC[args.workload]
+    vals = []
+    if args.workload == 'osem':
+        for _ in range(args.warmup + args.steps):
+            vals.append(cpu_osem_sample(params, seconds=6.0))
+    else:
+        from nipet_b200 import phantoms
+        lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
+        for _ in range(args.warmup + args.steps):
+            vals.append(cpu_hist_sample(lm, params))
+    vals = vals[args.warmup:]
+    v = float(np.mean([x['value'] for x in vals]))
+    cb = dict(vals[-1])
+    cb['value'] = v
+    return {'impl': 'reference', 'metric': metric, 'value': v, 'unit': unit, 'n_gpus': 0,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 / v if unit ==
+            'recon/s' else None, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': args.workload, 'implementation': 'FP64 oracle port, OpenMP'},
+            'cpu_baseline': cb, 'e2e': {'value': v, 'unit': unit, 'h2d_bytes_per_step': 0,
+                                        'd2h_bytes_per_step': 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='osem', choices=['osem', 'hist'])
+    ap.add_argument('--e2e-steps', type=int, default=1)
+    ap.add_argument('--events', type=int, default=200_000_000)
+    ap.add_argument('--duration', type=int, default=600)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+
+    if args.impl == 'reference':
+        out = run_reference(args)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+
+    import torch
+    ws, rank, local = _dist()
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    res = run_osem(args, ws, rank, dev) if args.workload == 'osem' else run_hist(args, ws, rank,
+                                                                                  dev)
+    metric, unit = METRIC[args.workload]
+    if rank == 0:
+        line = {'metric': metric, 'value': res['value'], 'unit': unit, 'n_gpus': ws,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms_per_step'],
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+                'dtype': 'f32' if args.workload == 'osem' else 'u32', 'data': 'synthetic',
+                'config': res['config'], 'roofline': res['roofline'],
+                'cpu_baseline': res.get('cpu_baseline'), 'e2e': res['e2e'],
+                'gpu_launches': res['gpu_launches'], 'clocks': res['clocks']}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

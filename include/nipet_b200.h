@@ -57,9 +57,10 @@ int nb_geom_destroy(nb_geom *g);
  * [naw][1807] uint8.  Replaces petprj.tprj (prj/src/prj_module.cu:70-224).  Synchronous. */
 int nb_geom_tables(nb_geom *g, float *tt, uint8_t *tv);
 
-/* Voxel-read count V of a forward projection over all LORs (direct: 1 per step,
- * oblique: 2 per step, 4 at an axial crossing), computed on the device.  Synchronous. */
-int nb_geom_count_reads(nb_geom *g, long long *reads);
+/* Voxel-read count V of a forward projection (direct: 1 per step, oblique: 2 per step,
+ * 4 at an axial crossing), computed on the device: the total over all LORs in *reads and,
+ * if per_lor (host [naw] int64) is not NULL, the count of every LOR.  Synchronous. */
+int nb_geom_count_reads(nb_geom *g, long long *per_lor, long long *reads);
 
 /* ---- projectors on the reference image layout [320][320][127] (y, x, z) ---------------
  * nb_fprj replaces petprj.fprj (prj/src/prj_module.cu:232-425 -> gpu_fprj, prjf.cu:209-320).
@@ -81,6 +82,12 @@ int nb_bprj(nb_geom *g, float *im, const float *sino, const int32_t *subs, int n
 int nb_fprj_col128(nb_geom *g, float *sino, const float *im128, const int32_t *subs, int nprj,
                    int span, int att, void *stream);
 int nb_bprj_col128(nb_geom *g, float *im128, const float *sino, const int32_t *subs, int nprj,
+                   int span, void *stream);
+/* Sensitivity image of a subset: sens128 = back projection of the rows subs[] of the
+ * full gap-free sinogram an (dev [68516][nsinos], e.g. attenuation x normalisation),
+ * i.e. what the reference computes with petprj.bprj(ansng[subs], subs)
+ * (prj/mmrrec.py:289-299).  sens128 is overwritten. */
+int nb_sens_col128(nb_geom *g, float *sens128, const float *an, const int32_t *subs, int nprj,
                    int span, void *stream);
 int nb_im_to_col128(float *im128, const float *im, int nimg, void *stream);
 int nb_col128_to_im(float *im, const float *im128, int nimg, void *stream);

@@ -34,11 +34,12 @@ SIGNATURES = {
     'nb_geom_create': ([I, P, I, P, I, P, P, P, P, I, C.POINTER(P)], I),
     'nb_geom_destroy': ([P], I),
     'nb_geom_tables': ([P, P, P], I),
-    'nb_geom_count_reads': ([P, C.POINTER(C.c_longlong)], I),
+    'nb_geom_count_reads': ([P, P, C.POINTER(C.c_longlong)], I),
     'nb_fprj': ([P, P, P, P, I, I, I, P], I),
     'nb_bprj': ([P, P, P, P, I, I, P], I),
     'nb_fprj_col128': ([P, P, P, P, I, I, I, P], I),
     'nb_bprj_col128': ([P, P, P, P, I, I, P], I),
+    'nb_sens_col128': ([P, P, P, P, I, I, P], I),
     'nb_im_to_col128': ([P, P, I, P], I),
     'nb_col128_to_im': ([P, P, I, P], I),
     'nb_geom_check': ([P, P], I),

@@ -70,7 +70,7 @@ __global__ void k_osem_update(float4 *__restrict__ img, float4 *__restrict__ bim
 // V: voxel reads of a full forward projection, one thread per (LOR, oblique pair)
 __global__ void k_count_reads(const float4 *__restrict__ hdr, const float *__restrict__ st,
                               const nb_ray *__restrict__ rays, int naw,
-                              unsigned long long *out) {
+                              unsigned long long *out, unsigned long long *per_lor) {
   const int lor = blockIdx.x;
   if (lor >= naw) return;
   const float4 h = hdr[lor];
@@ -91,6 +91,7 @@ __global__ void k_count_reads(const float4 *__restrict__ hdr, const float *__res
   }
   if (threadIdx.x == 0) tot += (unsigned long long)NB_NRINGS * n;
   atomicAdd(out, tot);
+  atomicAdd(per_lor + lor, tot);
 }
 
 template <int MODE, int CH>
@@ -184,6 +185,19 @@ extern "C" int nb_bprj_col128(nb_geom *g, float *im128, const float *sino, const
   return launch_project<MODE_BWD, CH_BWD>(g, a, (cudaStream_t)stream);
 }
 
+extern "C" int nb_sens_col128(nb_geom *g, float *sens128, const float *an, const int32_t *subs,
+                              int nprj, int span, void *stream) {
+  int st = check_common(g, nprj, subs, span);
+  if (st) return st;
+  NB_REQUIRE(sens128 && an, "nb_sens_col128: NULL image or sinogram");
+  NB_CUDA(cudaMemsetAsync(sens128, 0, sizeof(float) * NB_IMG_COL128, (cudaStream_t)stream));
+  PrjArgs a = base_args(g, subs, nprj, span);
+  a.bimg = sens128;
+  a.sino_in = an;
+  a.in_by_lor = 1;
+  return launch_project<MODE_BWD, CH_BWD>(g, a, (cudaStream_t)stream);
+}
+
 extern "C" int nb_fprj(nb_geom *g, float *sino, const float *im, const int32_t *subs, int nprj,
                        int span, int att, void *stream) {
   int st = check_common(g, nprj, subs, span);
@@ -238,15 +252,17 @@ extern "C" int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const f
   return NB_OK;
 }
 
-extern "C" int nb_geom_count_reads(nb_geom *g, long long *reads) {
+extern "C" int nb_geom_count_reads(nb_geom *g, long long *per_lor, long long *reads) {
   NB_REQUIRE(g && reads, "nb_geom_count_reads: NULL argument");
   NB_CUDA(cudaSetDevice(g->device));
   unsigned long long *d = nullptr;
-  NB_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
-  cudaMemset(d, 0, sizeof(unsigned long long));
-  k_count_reads<<<g->naw, 128>>>(g->d_hdr, g->d_st, g->d_rays, g->naw, d);
+  NB_CUDA(cudaMalloc(&d, sizeof(unsigned long long) * (1 + (size_t)g->naw)));
+  cudaMemset(d, 0, sizeof(unsigned long long) * (1 + (size_t)g->naw));
+  k_count_reads<<<g->naw, 128>>>(g->d_hdr, g->d_st, g->d_rays, g->naw, d, d + 1);
   unsigned long long h = 0;
   cudaError_t e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && per_lor)
+    e = cudaMemcpy(per_lor, d + 1, sizeof(long long) * g->naw, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_geom_count_reads", __FILE__, __LINE__);
   *reads = (long long)h;

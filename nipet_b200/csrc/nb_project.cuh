@@ -53,7 +53,8 @@ struct PrjArgs {
   const float *img;      // col128 image read by forward passes
   float *bimg;           // col128 image accumulated by backward passes
   float *sino;           // forward output [nprj][nout]
-  const float *sino_in;  // backward input [nprj][nout]
+  const float *sino_in;  // backward input [nprj][nout] (or [naw][nout] if in_by_lor)
+  int in_by_lor;         // backward: row of a LOR is its LOR index, not its subset position
   const uint16_t *psng;  // OSEM prompts [naw][nout]
   const float *rs;       // OSEM (r+s)/(an) [naw][nout]
   int fxbits;            // backward fixed point: |value| * 2^fxbits / 2^e fits every slot
@@ -303,7 +304,8 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
           if (ray < NB_NRAYS) {
             const nb_ray R = a.rays[ray];
             const int o = a.span == 11 ? R.out11 : R.out1;
-            const float bin = (MODE == MODE_BWD) ? a.sino_in[(size_t)J.p * nout + o] : rat[o];
+            const size_t row = a.in_by_lor ? (size_t)J.lor : (size_t)J.p;
+            const float bin = (MODE == MODE_BWD) ? a.sino_in[row * nout + o] : rat[o];
             v = bin * ray_s(a, ray, h.y);
           }
           S.acc[r] = v;

@@ -104,10 +104,14 @@ class Geometry:
                                             tv.ctypes.data_as(C.c_void_p)))
         return tt, tv
 
-    def count_reads(self) -> int:
+    def count_reads(self, per_lor: bool = False):
+        """Siddon voxel reads V of a full forward projection (and, if `per_lor`, the
+        [68516] int64 count of every LOR)."""
         v = C.c_longlong()
-        _lib.check(self._lib.nb_geom_count_reads(self.handle, C.byref(v)))
-        return v.value
+        arr = np.zeros(self.naw, dtype=np.int64) if per_lor else None
+        _lib.check(self._lib.nb_geom_count_reads(
+            self.handle, arr.ctypes.data_as(C.c_void_p) if per_lor else None, C.byref(v)))
+        return (v.value, arr) if per_lor else v.value
 
 
 _CACHE: dict = {}

@@ -92,6 +92,64 @@ def norm_sinogram(params: dict, eff: np.ndarray, span: int = 11) -> np.ndarray:
 # ---------------------------------------------------------------------------------------
 # list mode
 # ---------------------------------------------------------------------------------------
+def lm_stream_fast(n_events: int, duration_s: int, params: dict | None = None, seed: int = 0,
+                   device='cuda', delayed_frac: float = 0.2, tag_every_ms: int = 1,
+                   t0_ms: int = 1000, weights: str = 'phantom'):
+    """GPU version of `lm_stream` for benchmark-sized streams (returns a device int32
+    tensor).  With weights='phantom' prompt addresses are drawn proportional to the
+    attenuated span-1 forward projection of `brain_phantom(seed)`."""
+    import torch
+
+    from . import _lib
+    from .device import dev_ptr, get_geometry, stream_ptr
+    if params is None:
+        from .geometry import get_mmrparams
+        params = get_mmrparams()
+    dev = torch.device(device)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    live_aw = torch.from_numpy(
+        np.flatnonzero(params['txLUT']['msino'].T.reshape(-1) > 0).astype(np.int64)).to(dev)
+    n_del = int(round(n_events * delayed_frac))
+    n_pr = n_events - n_del
+    if weights == 'phantom':
+        geom = get_geometry(params['txLUT'], params['axLUT'], dev)
+        lib = _lib.load()
+        st = stream_ptr(dev)
+        x = torch.from_numpy(brain_phantom(seed)).to(dev)
+        mu = torch.from_numpy(water_mumap()).to(dev)
+        em = torch.empty((68516, 4084), device=dev)
+        at = torch.empty((68516, 4084), device=dev)
+        _lib.check(lib.nb_fprj(geom.handle, dev_ptr(em), dev_ptr(x), None, 68516, 1, 0, st))
+        _lib.check(lib.nb_fprj(geom.handle, dev_ptr(at), dev_ptr(mu), None, 68516, 1, 1, st))
+        w = (em * at).reshape(-1).double()
+        del em, at
+        cdf = torch.cumsum(w, 0)
+        del w
+        cdf /= cdf[-1].clone()
+        u = torch.rand(n_pr, generator=g, device=dev, dtype=torch.float64)
+        idx = torch.searchsorted(cdf, u).clamp_(max=cdf.numel() - 1)
+        del cdf, u
+        aw, sn1 = idx // 4084, idx % 4084
+        addr_p = sn1 * 86688 + live_aw[aw]
+    else:
+        addr_p = (torch.randint(0, 4084, (n_pr,), generator=g, device=dev) * 86688
+                  + live_aw[torch.randint(0, live_aw.numel(), (n_pr,), generator=g, device=dev)])
+    addr_d = (torch.randint(0, 4084, (n_del,), generator=g, device=dev) * 86688
+              + live_aw[torch.randint(0, live_aw.numel(), (n_del,), generator=g, device=dev)])
+    words = torch.cat([addr_p | (1 << 30), addr_d])
+    words = words[torch.randperm(words.numel(), generator=g, device=dev)]
+    n_ticks = duration_s * 1000 // tag_every_ms
+    ticks, _ = torch.sort(torch.randint(0, n_ticks, (words.numel(),), generator=g, device=dev))
+    counts = torch.bincount(ticks, minlength=n_ticks)
+    before = torch.cumsum(counts, 0) - counts
+    k = torch.arange(n_ticks, device=dev)
+    out = torch.empty(words.numel() + n_ticks, device=dev, dtype=torch.int64)
+    out[k + before] = 0x80000000 | (t0_ms + k * tag_every_ms)
+    out[torch.arange(words.numel(), device=dev) + ticks + 1] = words
+    out = torch.where(out >= 2**31, out - 2**32, out)
+    return out.to(torch.int32)
+
+
 def lm_stream(n_events: int, duration_s: int, span1_weights: np.ndarray | None = None,
               delayed_frac: float = 0.2, seed: int = 0, tag_every_ms: int = 1,
               t0_ms: int = 1000, params: dict | None = None,
