@@ -144,9 +144,9 @@ struct RayState {
   float acc[RPT];  // forward: line integral; backward: value to spread (bin * s * scale)
   float tzc[RPT];  // next axial crossing
   float dtz[RPT];
-  int zi[RPT];     // column slot of the current voxel
-  int dz[RPT];     // slot change at the next crossing
-  int dir[RPT];    // +1 / -1 (0: direct plane)
+  int zo[RPT];     // byte offset of the current voxel in its column (4 * slot)
+  int dz4[RPT];    // byte change of zo at the next crossing
+  int dir4[RPT];   // 4 * (+1 / -1), 0 for direct planes
   float tp;
 };
 
@@ -159,18 +159,18 @@ __device__ __forceinline__ void rays_init(const PrjArgs &a, const float4 h, RayS
     if (ray < NB_NRAYS) {
       nb_axial A;
       nb_axial_setup(a.rays[ray], h.y, h.x, h.z, A);
-      S.zi[r] = nb_zi(A.w);
+      S.zo[r] = 4 * nb_zi(A.w);
       S.tzc[r] = A.tzc;
       S.dtz[r] = A.dtz;
-      S.dir[r] = A.dir;
+      S.dir4[r] = 4 * A.dir;
       // slot change of the first crossing: parity of w decides (+64/-63 up, +63/-64 down)
-      S.dz[r] = A.dir > 0 ? ((A.w & 1) ? -63 : 64) : (A.dir < 0 ? ((A.w & 1) ? -64 : 63) : 0);
+      S.dz4[r] = 4 * (A.dir > 0 ? ((A.w & 1) ? -63 : 64) : (A.dir < 0 ? ((A.w & 1) ? -64 : 63) : 0));
     } else {
-      S.zi[r] = 127;  // padding slot, never crosses
+      S.zo[r] = 4 * 127;  // padding slot, never crosses
       S.tzc[r] = __int_as_float(0x7f800000);
       S.dtz[r] = 0.f;
-      S.dir[r] = 0;
-      S.dz[r] = 0;
+      S.dir4[r] = 0;
+      S.dz4[r] = 0;
     }
   }
 }
@@ -183,53 +183,99 @@ __device__ __forceinline__ float ray_s(const PrjArgs &a, int ray, float atn) {
   return __fsqrt_rn(__fmaf_rn(az_atn, az_atn, 1.0f));
 }
 
-// Forward walk over n steps of one chunk (prjf.cu:76-86 / :164-190).  The segment of a
-// step is [tp, min(tn, tzc)] in the current voxel and, at a crossing, [tzc, tn] in the
-// next one; a ray crosses at most one z plane per step, as in the reference.
-__device__ __forceinline__ void walk_fwd(RayState &S, const float *col0, const float *tnb, int n) {
-  float tp = S.tp;
-  for (int i = 0; i < n; ++i) {
-    const float tn = tnb[i];
-    const float *col = col0 + i * NB_COLW;
-#pragma unroll
-    for (int r = 0; r < RPT; r++) {
-      const float tz = S.tzc[r];
-      const float v0 = col[S.zi[r]];
-      const float fa = __fsub_rn(fminf(tn, tz), tp);
-      S.acc[r] = fmaf(fa, v0, S.acc[r]);
-      if (tn > tz) {
-        S.zi[r] += S.dz[r];
-        S.dz[r] = S.dir[r] - S.dz[r];
-        S.acc[r] = fmaf(__fsub_rn(tn, tz), col[S.zi[r]], S.acc[r]);
-        S.tzc[r] = __fadd_rn(tz, S.dtz[r]);
-      }
-    }
-    tp = tn;
-  }
-  S.tp = tp;
+// Shared-memory accessors on 32-bit shared-window addresses (the per-ray cursors below).
+static __device__ __forceinline__ float lds_f32(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+static __device__ __forceinline__ void reds_add_s32(uint32_t addr, int v) {
+  asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
-// Backward walk (prjb.cu:70-77 / :153-178): the same segments, spread as int32 fixed point.
-__device__ __forceinline__ void walk_bwd(RayState &S, int *col0, const float *tnb, int n) {
+// One step of a ray, forward (prjf.cu:76-86 / :164-190).  The step covers [tp, tn]; a ray
+// that crosses a z plane at tzc inside it (at most one per step, as in the reference)
+// integrates [tp, tzc] in its current voxel v0 and [tzc, tn] in the next voxel v1, i.e.
+// lt*v0 + (tn - tzc)*(v1 - v0).  `cur` is the ray's shared-memory cursor: the address of
+// its voxel in the chunk's first column; step u of the chunk adds u*512 bytes.
+static __device__ __forceinline__ void step_fwd(float &acc, uint32_t &cur, int &dz4, float &tzc,
+                                                const int dir4, const float dtz, float tn, float lt,
+                                                uint32_t off) {
+  const float v0 = lds_f32(cur + off);
+  acc = fmaf(lt, v0, acc);
+  if (tn > tzc) {
+    cur += dz4;
+    dz4 = dir4 - dz4;
+    const float v1 = lds_f32(cur + off);
+    acc = fmaf(__fsub_rn(tn, tzc), v1 - v0, acc);
+    tzc = __fadd_rn(tzc, dtz);
+  }
+}
+
+// One step of a ray, backward (prjb.cu:70-77 / :153-178): the same segments, spread as
+// int32 fixed point (acc holds the ray's value times the per-LOR scale).
+static __device__ __forceinline__ void step_bwd(const float acc, uint32_t &cur, int &dz4,
+                                                float &tzc, const int dir4, const float dtz,
+                                                float tn, float tp, float lt, uint32_t off) {
+  if (tn > tzc) {
+    reds_add_s32(cur + off, __float2int_rn(__fsub_rn(tzc, tp) * acc));
+    cur += dz4;
+    dz4 = dir4 - dz4;
+    reds_add_s32(cur + off, __float2int_rn(__fsub_rn(tn, tzc) * acc));
+    tzc = __fadd_rn(tzc, dtz);
+  } else {
+    reds_add_s32(cur + off, __float2int_rn(lt * acc));
+  }
+}
+
+// Walk n steps of one shared-memory chunk (column i at chunk + i*512 bytes).  Steps are
+// processed 8 at a time with immediate column offsets (the exit parameters come as two
+// 16-byte loads), then one at a time for the tail.
+template <bool BWD>
+__device__ __forceinline__ void walk_chunk(RayState &S, const void *chunk, const float *tnb,
+                                           int n) {
+  const uint32_t sb = nb_smem_u32(chunk);
+  uint32_t cur[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; r++) cur[r] = sb + (uint32_t)S.zo[r];
   float tp = S.tp;
-  for (int i = 0; i < n; ++i) {
+  int i = 0;
+  for (; i + 8 <= n; i += 8) {
+    const float4 ta = *reinterpret_cast<const float4 *>(tnb + i);
+    const float4 tb = *reinterpret_cast<const float4 *>(tnb + i + 4);
+    const float t8[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const float tn = t8[u];
+      const float lt = __fsub_rn(tn, tp);
+#pragma unroll
+      for (int r = 0; r < RPT; r++) {
+        if (BWD)
+          step_bwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, tp, lt, u * 512u);
+        else
+          step_fwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, lt, u * 512u);
+      }
+      tp = tn;
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; r++) cur[r] += 8 * 512;
+  }
+  for (; i < n; i++) {
     const float tn = tnb[i];
-    int *col = col0 + i * NB_COLW;
+    const float lt = __fsub_rn(tn, tp);
 #pragma unroll
     for (int r = 0; r < RPT; r++) {
-      const float tz = S.tzc[r];
-      const float fa = __fsub_rn(fminf(tn, tz), tp);
-      atomicAdd(col + S.zi[r], __float2int_rn(fa * S.acc[r]));
-      if (tn > tz) {
-        S.zi[r] += S.dz[r];
-        S.dz[r] = S.dir[r] - S.dz[r];
-        atomicAdd(col + S.zi[r], __float2int_rn(__fsub_rn(tn, tz) * S.acc[r]));
-        S.tzc[r] = __fadd_rn(tz, S.dtz[r]);
-      }
+      if (BWD)
+        step_bwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, tp, lt, 0u);
+      else
+        step_fwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, lt, 0u);
+      cur[r] += 512;
     }
     tp = tn;
   }
   S.tp = tp;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) S.zo[r] = (int)(cur[r] - sb) - n * (NB_COLW * 4);
 }
 
 template <int MODE, int CH>
@@ -333,11 +379,11 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
     if (load) {
       if (!nb_mbar_wait(&bars[b], (phase >> b) & 1u, WAIT_POLLS)) atomicExch(sflag, 1);
       phase ^= 1u << b;
-      walk_fwd(S, fb, tb, n);
+      walk_chunk<false>(S, fb, tb, n);
     } else {
       // the bulk reduce that last read staging buffer b must be done before we refill it
       if (warp0) nb_bulk_wait_read<1>();
-      walk_bwd(S, ib, tb, n);
+      walk_chunk<true>(S, ib, tb, n);
       __syncthreads();
       // int32 accumulators -> float staging (and back to zero for their next use)
       const int nv = n * NB_COLW / 4;

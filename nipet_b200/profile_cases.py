@@ -1,0 +1,70 @@
+"""Small, self-contained GPU cases for profiling the hot kernels with Nsight Compute.
+
+    python -m nipet_b200.profile_cases projectors   # k_project: back, forward, fused OSEM
+    python -m nipet_b200.profile_cases hist         # k_hist on a 20M-word stream
+
+`projectors` builds the geometry, a phantom image (col128 layout), subset 3 of 14 and random
+prompt / (r+s)/(an) / a*n sinograms (~0.8 GB on the device), then launches the back projection
+(sensitivity), forward projection and fused OSEM sub-iteration six times each, so the k_project
+launches 15, 16, 17 are one warm launch of each mode:
+
+    ncu --set full --clock-control none -k regex:k_project -s 15 -c 3 -o prof \\
+        python -m nipet_b200.profile_cases projectors
+
+`hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2).
+"""
+from __future__ import annotations
+
+import sys
+
+import torch
+
+
+def projectors(device='cuda:0'):
+    from . import _lib, geometry, petprj, phantoms
+    from .device import dev_ptr, get_geometry, stream_ptr
+    dev = torch.device(device)
+    p = geometry.get_mmrparams()
+    g = get_geometry(p['txLUT'], p['axLUT'], dev)
+    lib = _lib.load()
+    st = stream_ptr(dev)
+    img = petprj.to_col128(torch.from_numpy(phantoms.brain_phantom(0)).to(dev)).reshape(-1)
+    subs = torch.from_numpy(geometry.get_subsets14(3, p)[0]).to(dev)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    an = torch.rand((68516, 837), device=dev, generator=gen) + 0.5
+    psng = torch.randint(0, 8, (68516, 837), device=dev, generator=gen).to(torch.int32).to(
+        torch.uint16)
+    rs = torch.full((68516, 837), 0.01, device=dev)
+    msk = torch.ones(320 * 320 * 128, device=dev, dtype=torch.uint8)
+    sens = torch.empty(320 * 320 * 128, device=dev)
+    bimg = torch.empty_like(sens)
+    sino = torch.empty((subs.numel(), 837), device=dev)
+    n = subs.numel()
+    for _ in range(6):
+        _lib.check(lib.nb_sens_col128(g.handle, dev_ptr(sens), dev_ptr(an), dev_ptr(subs), n, 11,
+                                      st))
+        _lib.check(lib.nb_fprj_col128(g.handle, dev_ptr(sino), dev_ptr(img), dev_ptr(subs), n, 11,
+                                      0, st))
+        _lib.check(lib.nb_osem_subset(g.handle, dev_ptr(img), dev_ptr(bimg), dev_ptr(sens),
+                                      dev_ptr(msk), dev_ptr(psng), dev_ptr(rs), dev_ptr(subs), n,
+                                      st))
+    torch.cuda.synchronize(dev)
+    g.check()
+    print('projectors ok')
+
+
+def hist(device='cuda:0'):
+    from . import geometry, mmr_lmproc, phantoms
+    dev = torch.device(device)
+    p = geometry.get_mmrparams()
+    lm = phantoms.lm_stream_fast(20_000_000, 60, params=p, seed=0, device=dev)
+    pl = mmr_lmproc.plan(lm.cpu().numpy())
+    Cnt = dict(p['Cnt'], SPN=11, BTP=0)
+    for _ in range(3):
+        r = mmr_lmproc.hist_stream(lm, p['txLUT'], p['axLUT'], Cnt, pl=pl, unpack=False)
+    torch.cuda.synchronize(dev)
+    print('hist ok', int(r['phc'].sum()))
+
+
+if __name__ == '__main__':
+    {'projectors': projectors, 'hist': hist}[sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
