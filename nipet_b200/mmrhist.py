@@ -1,0 +1,77 @@
+"""Stand-in for NIPET's `lm/mmrhist.py` histogramming front end: `mmrhist` and `hist`
+(`mmrhist.py:25-180`), on the GPU histogrammer (`mmr_lmproc`)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import scipy.ndimage as ndi
+
+from . import mmr_lmproc
+
+__all__ = ['mmrhist', 'hist']
+
+
+def mmrhist(datain, scanner_params, t0=0, t1=0, outpath='', frms=None, use_stored=False,
+            store=False, cmass_sig=5):
+    """List-mode histogram, head curves and centre of mass (`mmrhist.py:25-37`)."""
+    return hist(datain, scanner_params['txLUT'], scanner_params['axLUT'],
+                scanner_params['Cnt'], t0=t0, t1=t1, cmass_sig=cmass_sig, frms=frms,
+                use_stored=use_stored, store=store, outpath=outpath)
+
+
+def hist(datain, txLUT, axLUT, Cnt, t0=0, t1=0, cmass_sig=5, frms=None, use_stored=False,
+         store=False, outpath=''):
+    """`mmrhist.py:40-180`: returns the reference's output dict (`phc`, `dhc`, `cmass`,
+    `pvs_sgtl`, `pvs_crnl`, `fansums`, `sngl_rate`, `tsngl`, `buckets`, `psino`, `dsino`,
+    `pssr`, `t0`, `t1`, `dur`)."""
+    nsinos = {1: Cnt['NSN1'], 11: Cnt['NSN11'], 0: Cnt['NSEG0']}[Cnt['SPN']]
+    fname = f"sinos_s{Cnt['SPN']}_frm-{t0}-{t1}.npz"
+    if use_stored and 'sinos' in datain and os.path.basename(datain['sinos']) == fname:
+        hstout = dict(np.load(datain['sinos'], allow_pickle=True))
+        nitag = len(hstout['phc'])
+    elif os.path.isfile(datain['lm_bf']):
+        nele, ttags, tpos = mmr_lmproc.lminfo(datain['lm_bf'])
+        nitag = int((ttags[1] - ttags[0] + 999) / 1000)
+        if t1 > nitag:
+            t1 = nitag
+        if t0 >= nitag:
+            raise ValueError('the time frame definition is not allowed! '
+                             '(outside acquisition time)')
+        tn = int(5400 / 4) if nitag > 5400 else int((nitag + 3) / 4)
+        hstout = {
+            'phc': np.zeros(nitag, np.uint32), 'dhc': np.zeros(nitag, np.uint32),
+            'mss': np.zeros(nitag, np.float32),
+            'pvs': np.zeros((tn, Cnt['NSEG0'], Cnt['NSBINS']), np.uint32),
+            'bck': np.zeros((2, nitag, Cnt['NBCKT']), np.uint32),
+            'fan': np.zeros((Cnt['NRNG'], Cnt['NCRS']), np.uint32),
+            'psn': np.zeros((nsinos, Cnt['NSANGLES'], Cnt['NSBINS']), np.uint16),
+            'dsn': np.zeros((nsinos, Cnt['NSANGLES'], Cnt['NSBINS']), np.uint16),
+            'ssr': np.zeros((Cnt['NSEG0'], Cnt['NSANGLES'], Cnt['NSBINS']), np.uint32)}
+        mmr_lmproc.hist(hstout, datain['lm_bf'], t0, t1, txLUT, axLUT, Cnt)
+        if store:
+            d = os.path.dirname(datain['lm_bf']) if outpath == '' else os.path.join(outpath,
+                                                                                  'sino')
+            os.makedirs(d, exist_ok=True)
+            np.savez(os.path.join(d, fname), **hstout)
+    else:
+        raise FileNotFoundError('input list-mode data is not defined')
+
+    pvs_sgtl = np.right_shift(hstout['pvs'], 8).astype(np.float32)
+    pvs_crnl = np.bitwise_and(hstout['pvs'], 255).astype(np.float32)
+    cmass = Cnt['SO_VXZ'] * ndi.gaussian_filter(hstout['mss'], cmass_sig, mode='mirror')
+    nsr = hstout['bck'][1, :, :] >> 30
+    bck0 = hstout['bck'][0].copy()
+    bck0[nsr > 0] = bck0[nsr > 0] / nsr[nsr > 0]
+    tmsk = np.sum(nsr, axis=1) > 0
+    single_rate = np.copy(bck0[tmsk, :])
+    t = np.arange(nitag)[tmsk]
+    buckets = (np.int32(np.sum(single_rate, axis=0) / single_rate.shape[0])
+               if single_rate.shape[0] else np.zeros(Cnt['NBCKT'], np.int32))
+    if t0 == t1:
+        t1 = t0 + nitag
+    return {'t0': t0, 't1': t1, 'dur': t1 - t0, 'phc': hstout['phc'], 'dhc': hstout['dhc'],
+            'cmass': cmass, 'pvs_sgtl': pvs_sgtl, 'pvs_crnl': pvs_crnl,
+            'fansums': hstout['fan'], 'sngl_rate': single_rate, 'tsngl': t,
+            'buckets': buckets, 'psino': hstout['psn'].astype(np.uint16),
+            'dsino': hstout['dsn'].astype(np.uint16), 'pssr': hstout['ssr']}
