@@ -151,6 +151,26 @@ int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag, cons
             uint32_t *psino, uint32_t *ssrb, uint32_t *phc, uint32_t *dhc, int32_t *zR,
             int32_t *zM, uint32_t *pvs, uint32_t *fan, uint32_t *bck, void *stream);
 
+/* nb_hist_static has no counterpart in the reference.  It is nb_hist for callers that
+ * cannot allocate device memory: for example an acquisition loop that histograms each
+ * incoming list-mode buffer while the scan runs, where a device allocation could fail or
+ * stall the stream mid-acquisition, or a host process whose device memory is entirely
+ * owned by another allocator.  Same arguments, semantics and outputs as nb_hist; it makes
+ * no allocation: the look-up tables and chunk plan are staged in a file-scope static
+ * device array of 512 KiB that every GPU loading this library keeps until exit.
+ * Limits: at most 4096 chunks in the plan (about 5e10 words); larger plans are rejected
+ * with NB_ERR_ARG.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress, with the device current) and caches it, so make that first call
+ * before any stream capture.  All calls on a device share the array and it keeps the last
+ * call's tables; calls that overlap on the GPU race on it and must be serialised. */
+int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag,
+                   const int *ele4chnk, const int *ele4thrd, int toff, int nitag, int tstart,
+                   int tstop, int span, int btp, double btprt, uint64_t seed, int rep0, int nrep,
+                   const int16_t *sn1_sn11, const int16_t *sn1_ssrb, const int16_t *sn1_rno,
+                   const int16_t *s2cF, uint32_t *psino, uint32_t *ssrb, uint32_t *phc,
+                   uint32_t *dhc, int32_t *zR, int32_t *zM, uint32_t *pvs, uint32_t *fan,
+                   uint32_t *bck, void *stream);
+
 /* Split packed sinograms: psn = w & 0xFFFF, dsn = w >> 16 (lmproc.cu:162-168), and the
  * prompt/delayed totals (host, may be NULL).  Synchronous. */
 int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t *dsn,

@@ -52,6 +52,8 @@ SIGNATURES = {
                     C.POINTER(I), C.POINTER(I)], I),
     'nb_hist': ([P, C.c_int64, I, P, P, P, I, I, I, I, I, I, C.c_double, C.c_uint64, I, I, P, P,
                  P, P, P, P, P, P, P, P, P, P, P, P], I),
+    'nb_hist_static': ([P, C.c_int64, I, P, P, P, I, I, I, I, I, I, C.c_double, C.c_uint64, I, I,
+                        P, P, P, P, P, P, P, P, P, P, P, P, P, P], I),
     'nb_hist_unpack':([P, C.c_size_t, P, P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                         P], I),
 }

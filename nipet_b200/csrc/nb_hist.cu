@@ -504,3 +504,156 @@ extern "C" int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn
   if (dsum) *dsum = h[1];
   return NB_OK;
 }
+
+// ---------------------------------------------------------------------------------------
+// nb_hist_static: nb_hist for callers that cannot allocate device memory.
+//
+// nb_hist stages its look-up tables and chunk plan in a stream-ordered device allocation
+// made on every call.  This variant stages them instead in one file-scope static device
+// array (NB_HIST_STATIC_BYTES, holding at most NB_HIST_STATIC_MAX_CHUNKS chunks), so a call
+// makes no allocation of any kind: only cudaMemcpyAsync copies from the caller's host
+// arrays into that array and the kernel launch.  The array belongs to every GPU that loads
+// this library until the process exits; all calls on a device share it and it keeps the
+// last call's tables, which every call overwrites before its kernel reads them (nothing in
+// it has to start at zero).  Calls that overlap on the GPU (different streams, or other
+// host threads) race on the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------------------
+#include <mutex>
+
+#define NB_HIST_STATIC_MAX_CHUNKS 4096
+#define NB_HIST_STATIC_BYTES (512u * 1024u)
+
+static __device__ __align__(256) unsigned char g_hist_static_scratch[NB_HIST_STATIC_BYTES];
+
+namespace {
+constexpr size_t kLutOff = 0;
+constexpr size_t kS2cOff = (sizeof(HistLUT) + 255) & ~(size_t)255;
+constexpr size_t kAtagOff = (kS2cOff + (size_t)NB_NSBINANG * sizeof(short2) + 255) & ~(size_t)255;
+constexpr size_t kE4cOff = kAtagOff + sizeof(int64_t) * NB_HIST_STATIC_MAX_CHUNKS;
+constexpr size_t kE4tOff = kE4cOff + sizeof(int) * NB_HIST_STATIC_MAX_CHUNKS;
+constexpr size_t kStaticEnd = kE4tOff + sizeof(int) * NB_HIST_STATIC_MAX_CHUNKS;
+static_assert(kStaticEnd <= NB_HIST_STATIC_BYTES, "static histogram scratch too small");
+
+std::mutex g_static_mu;
+unsigned char *g_static_addr[64] = {};
+
+// Device address of the static array on the current device.  The host-side name of a
+// __device__ variable is only a stand-in, so the address is looked up once per device
+// (on the first call there, with that device current) and cached.
+int static_scratch(unsigned char **out) {
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_REQUIRE(dev >= 0 && dev < 64, "nb_hist_static: device index above 63");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_hist_static_scratch);
+    if (e != cudaSuccess)
+      return nb_cuda_fail(e, "cudaGetSymbolAddress(histogram static scratch)", __FILE__,
+                          __LINE__);
+    g_static_addr[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_static_addr[dev];
+  return NB_OK;
+}
+}  // namespace
+
+extern "C" int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag,
+                              const int *ele4chnk, const int *ele4thrd, int toff, int nitag,
+                              int tstart, int tstop, int span, int btp, double btprt,
+                              uint64_t seed, int rep0, int nrep, const int16_t *sn1_sn11,
+                              const int16_t *sn1_ssrb, const int16_t *sn1_rno,
+                              const int16_t *s2cF, uint32_t *psino, uint32_t *ssrb,
+                              uint32_t *phc, uint32_t *dhc, int32_t *zR, int32_t *zM,
+                              uint32_t *pvs, uint32_t *fan, uint32_t *bck, void *stream) {
+  NB_REQUIRE(lm && atag && ele4chnk && ele4thrd, "nb_hist_static: NULL stream or plan");
+  NB_REQUIRE(sn1_sn11 && sn1_ssrb && sn1_rno && s2cF, "nb_hist_static: NULL LUT");
+  NB_REQUIRE(psino && ssrb && phc && dhc && zR && zM && pvs && fan && bck,
+             "nb_hist_static: NULL output");
+  NB_REQUIRE(span == 0 || span == 1 || span == 11, "nb_hist_static: span must be 0, 1 or 11");
+  NB_REQUIRE(btp >= 0 && btp <= 2, "nb_hist_static: btp must be 0, 1 or 2");
+  NB_REQUIRE(nrep >= 1 && nitag > 0 && nchnk >= 0, "nb_hist_static: bad sizes");
+  NB_REQUIRE(!(btp == 2 && !(btprt > 0)), "nb_hist_static: btprt must be > 0");
+  if (nchnk > NB_HIST_STATIC_MAX_CHUNKS) {
+    nb_set_error_msg("nb_hist_static: the chunk plan has %d chunks, but the static scratch holds "
+                     "at most %d (use nb_hist)", nchnk, NB_HIST_STATIC_MAX_CHUNKS);
+    return NB_ERR_ARG;
+  }
+  for (int n = 0; n < nchnk; n++) {
+    NB_REQUIRE(atag[n] >= 0 && ele4chnk[n] >= 0 && atag[n] + ele4chnk[n] <= ele,
+               "nb_hist_static: chunk outside the stream");
+    NB_REQUIRE(ele4thrd[n] >= 0, "nb_hist_static: bad slice length");
+  }
+  for (int i = 0; i < NB_NSN1; i++)
+    NB_REQUIRE(sn1_sn11[i] >= 0 && sn1_sn11[i] < NB_NSN11 && sn1_ssrb[i] >= 0 &&
+                   sn1_ssrb[i] < NB_SEG0 && sn1_rno[2 * i] >= 0 && sn1_rno[2 * i] < NB_NRINGS &&
+                   sn1_rno[2 * i + 1] >= 0 && sn1_rno[2 * i + 1] < NB_NRINGS,
+               "nb_hist_static: axial LUT out of range");
+  if (nchnk == 0) return NB_OK;
+  unsigned char *base = nullptr;
+  int st = static_scratch(&base);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+
+  HistArgs a{};
+  a.lm = lm;
+  a.nchnk = nchnk;
+  a.toff = toff;
+  a.nitag = nitag;
+  a.tstart = tstart;
+  a.tstop = tstop;
+  a.span = span;
+  a.btp = btp;
+  a.seed = seed;
+  a.rep0 = rep0;
+  a.nrep = nrep;
+  poisson_thresholds(btp == 2 ? btprt : 1.0, a.thr);
+  a.nbins = span == 1 ? 354033792ull : (span == 11 ? 72557856ull : (size_t)NB_SEG0 * NB_NSBINANG);
+  const int tn = nitag > NB_MXNITAG ? NB_MXNITAG : nitag;
+  a.sne = (size_t)((tn + 3) / 4) * NB_SEG0 * NB_NSBINS;
+  a.psino = psino;
+  a.ssrb = ssrb;
+  a.phc = phc;
+  a.dhc = dhc;
+  a.zR = zR;
+  a.zM = zM;
+  a.pvs = pvs;
+  a.fan = fan;
+  a.bck = bck;
+  a.lut = reinterpret_cast<const HistLUT *>(base + kLutOff);
+  a.s2cF = reinterpret_cast<const short2 *>(base + kS2cOff);
+  a.atag = reinterpret_cast<const int64_t *>(base + kAtagOff);
+  a.e4c = reinterpret_cast<const int *>(base + kE4cOff);
+  a.e4t = reinterpret_cast<const int *>(base + kE4tOff);
+  const size_t nsn = (size_t)NB_NSN1 * sizeof(int16_t);
+  cudaError_t e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_sn11), sn1_sn11, nsn,
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_ssrb), sn1_ssrb, nsn,
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_rno), sn1_rno, 2 * nsn,
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kS2cOff, s2cF, (size_t)NB_NSBINANG * sizeof(short2),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kAtagOff, atag, sizeof(int64_t) * nchnk, cudaMemcpyHostToDevice,
+                        s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kE4cOff, ele4chnk, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base + kE4tOff, ele4thrd, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nslices = nchnk * NB_TOTHRDS;
+    int blocks = (nslices + 7) / 8;
+    if (blocks > nsm * 8) blocks = nsm * 8;
+    k_hist<<<blocks, 256, 0, s>>>(a);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist_static", __FILE__, __LINE__);
+  return NB_OK;
+}

@@ -70,3 +70,16 @@ def test_lm_plan_rejects_streams_without_tags():
                         a.ctypes.data_as(C.c_void_p), e.ctypes.data_as(C.c_void_p),
                         e.ctypes.data_as(C.c_void_p), *[C.byref(o) for o in out])
     assert st == 6 and b'time tag' in lib.nb_last_error()
+
+
+def test_hist_static_rejects_oversized_plan_on_host():
+    lib = _lib.load()
+    n = 5000
+    z64 = np.zeros(n + 1, np.int64)
+    z32 = np.zeros(n, np.int32)
+    lut = np.zeros(86688 * 2, np.int16)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    dummy = C.c_void_p(16)
+    st = lib.nb_hist_static(dummy, 10, n, p(z64), p(z32), p(z32), 0, 1, 0, 1, 11, 0, 1.0, 0, 0,
+                            1, p(lut), p(lut), p(lut), p(lut), *([dummy] * 9), None)
+    assert st == 1 and b'4096' in lib.nb_last_error()
