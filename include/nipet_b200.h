@@ -123,6 +123,26 @@ int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens1
                    const uint8_t *msk128, const uint16_t *psng, const float *rs,
                    const int32_t *subs, int nprj, void *stream);
 
+/* ---- batched OSEM: many images (bootstrap replicates, dynamic frames) per launch --------
+ * The reference reconstructs one image per osem() call (recon.cu:318-521); these entry
+ * points run one sub-iteration for nrep images that share geometry, attenuation,
+ * normalisation and sensitivity, each with its own prompts:
+ *   img, bimg  dev [ceil(nrep/bs)][320*320][128][bs] float ("col128 x bs" layout: the bs
+ *              images of a group interleaved per voxel); img updated in place, bimg scratch
+ *              (left zeroed)
+ *   sens128    dev col128 sensitivity image of this subset; msk128 dev col128 uint8 mask
+ *   psng       dev [nrep][68516][nsinos] uint16 prompts; rs dev [68516][nsinos] float
+ *              (r+s)/(an) from nb_osem_rs; rscale dev [nrep] per-image randoms factor
+ *   bs         1, 2 or 4 (4: span 11 only); span 11 (837 sinograms) or 1 (4084)
+ * nb_to_batch / nb_from_batch convert nrep reference-layout images [nrep][320][320][127]
+ * to and from that layout. */
+int nb_to_batch(float *dst, const float *src, int nrep, int bs, void *stream);
+int nb_from_batch(float *dst, const float *src, int nrep, int bs, void *stream);
+int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens128,
+                         const uint8_t *msk128, const uint16_t *psng, const float *rs,
+                         const float *rscale, int nrep, int bs, int span, const int32_t *subs,
+                         int nprj, void *stream);
+
 /* ---- list-mode histogramming (lm/src/lmproc.cu:12-230, hst.cu:37-528, lmaux.cu:17-270) -
  * nb_lm_plan replaces getLMinfo + modifyLMinfo: the chunk plan of a list-mode stream
  * (host [ele] int32 words), chunks cut at time tags with t % 100 ms == 0, and the time

@@ -1,0 +1,210 @@
+"""Batched OSEM: many bootstrap replicates or dynamic frames reconstructed together.
+
+All images share the scanner geometry, attenuation x normalisation (a*n) and hence the
+per-subset sensitivity images; each has its own prompts and a randoms level
+(`rscale[b]` times a common (r+s)/(an) sinogram).  One sub-iteration of all images is one
+persistent kernel launch (`nb_osem_batch_subset`), and a full iteration (14 sub-iterations)
+can be captured once as a CUDA graph and replayed.  The batch width `bs` (images sharing
+one walk of the Siddon geometry) is chosen by `autotune` by timing the candidates on the
+device, and cached per device.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib, geometry
+from .device import dev_ptr, get_geometry, stream_ptr
+from .mmrrec import subset_table
+from .petprj import COL128, to_col128
+
+__all__ = ['BatchRecon', 'autotune', 'bootstrap_prompts']
+
+NAW = 68516
+_TUNE_CACHE: dict = {}
+
+
+def bootstrap_prompts(mean: torch.Tensor, totals, seed: int = 0) -> torch.Tensor:
+    """[len(totals), 68516, nsinos] uint16 Poisson replicates of a noise-free mean
+    sinogram, replicate b scaled to an expected total of `totals[b]` counts."""
+    base = float(mean.double().sum())
+    out = torch.empty((len(totals),) + tuple(mean.shape), device=mean.device, dtype=torch.uint16)
+    g = torch.Generator(device=mean.device).manual_seed(seed)
+    for b, t in enumerate(totals):
+        y = torch.poisson(mean * (float(t) / base), generator=g)
+        out[b] = y.clamp_(max=65535).to(torch.int32).to(torch.uint16)
+    return out
+
+
+class BatchRecon:
+    """OSEM for `nrep` images on one device (span 11 or 1, PSF off)."""
+
+    def __init__(self, params: dict, psng: torch.Tensor, rs: torch.Tensor, an: torch.Tensor,
+                 rscale=None, device=None, span: int = 11, bs: int | None = None,
+                 nsub: int = 14, mask_radius: float = 29.0):
+        self.device = torch.device(device or psng.device)
+        self.params = params
+        self.span = int(span)
+        self.nout = 837 if self.span == 11 else 4084
+        self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
+        self.lib = _lib.load()
+        dev = self.device
+        if psng.dtype != torch.uint16 or psng.dim() != 3 or tuple(psng.shape[1:]) != (NAW,
+                                                                                      self.nout):
+            raise ValueError(f'psng must be uint16 [nrep, {NAW}, {self.nout}]')
+        self.psng = psng.to(dev).contiguous()
+        self.nrep = int(psng.shape[0])
+        self.rs = rs.to(dev, torch.float32).contiguous()
+        self.an = an.to(dev, torch.float32).contiguous()
+        rsc = np.ones(self.nrep, np.float32) if rscale is None else np.asarray(rscale, np.float32)
+        self.rscale = torch.from_numpy(rsc).to(dev)
+        tab = subset_table(params, nsub)
+        self.nsub, self.nprj = tab.shape[0], int(tab[0, 0])
+        self.subs = [torch.from_numpy(tab[i, 1:]).to(dev) for i in range(self.nsub)]
+        msk = geometry.get_cylinder(params['Cnt'], rad=mask_radius, xo=0, yo=0, unival=1,
+                                    gpu_dim=True) > 0.9
+        self.msk128 = (to_col128(torch.from_numpy(msk.astype(np.float32)).to(dev)) > 0.5).to(
+            torch.uint8).reshape(-1)
+        self.sens128 = torch.empty((self.nsub, COL128), device=dev)
+        self.graph = None
+        self.launches = 0
+        self.bs = int(bs) if bs else autotune(self)
+        self._alloc()
+
+    def _alloc(self):
+        ng = (self.nrep + self.bs - 1) // self.bs
+        self.img = torch.empty(ng * COL128 * self.bs, device=self.device)
+        self.bimg = torch.zeros_like(self.img)
+        self.graph = None
+
+    # -------------------------------------------------------------------------------------
+    def sensitivity(self):
+        st = stream_ptr(self.device)
+        for i in range(self.nsub):
+            _lib.check(self.lib.nb_sens_col128(self.geom.handle, dev_ptr(self.sens128[i]),
+                                               dev_ptr(self.an), dev_ptr(self.subs[i]),
+                                               self.nprj, self.span, st))
+            self.launches += 1
+
+    def init_images(self, value: float = 1.0):
+        ones = torch.full((self.nrep, 320, 320, 127), value, device=self.device)
+        _lib.check(self.lib.nb_to_batch(dev_ptr(self.img), dev_ptr(ones), self.nrep, self.bs,
+                                        stream_ptr(self.device)))
+        self.launches += 1
+
+    def subiteration(self, i: int, stream=None):
+        st = stream if stream is not None else stream_ptr(self.device)
+        _lib.check(self.lib.nb_osem_batch_subset(
+            self.geom.handle, dev_ptr(self.img), dev_ptr(self.bimg), dev_ptr(self.sens128[i]),
+            dev_ptr(self.msk128), dev_ptr(self.psng), dev_ptr(self.rs), dev_ptr(self.rscale),
+            self.nrep, self.bs, self.span, dev_ptr(self.subs[i]), self.nprj, st))
+        self.launches += 2
+
+    def iteration(self, use_graph: bool = True):
+        """One OSEM iteration (all subsets) for all images; replayed from a CUDA graph after
+        the first call when `use_graph`."""
+        if not use_graph:
+            for i in range(self.nsub):
+                self.subiteration(i)
+            return
+        if self.graph is None:
+            # warm-up on a side stream (required before capture), then capture
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                snap = self.img.clone()
+                for i in range(self.nsub):
+                    self.subiteration(i, C_stream(s))
+                self.img.copy_(snap)
+                del snap
+                with torch.cuda.graph(g, stream=s):
+                    for i in range(self.nsub):
+                        self.subiteration(i, C_stream(s))
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self.graph = g
+        self.graph.replay()
+        self.launches += 2 * self.nsub
+
+    def run(self, niter: int = 4, use_graph: bool = True, with_sensitivity: bool = True):
+        if with_sensitivity:
+            self.sensitivity()
+        self.init_images()
+        for _ in range(niter):
+            self.iteration(use_graph)
+        return self
+
+    def images(self) -> torch.Tensor:
+        out = torch.empty((self.nrep, 320, 320, 127), device=self.device)
+        _lib.check(self.lib.nb_from_batch(dev_ptr(out), dev_ptr(self.img), self.nrep, self.bs,
+                                          stream_ptr(self.device)))
+        return out
+
+    def mean_std(self):
+        """Voxel-wise mean and standard deviation (ddof=1) over the images."""
+        x = self.images().double()
+        return x.mean(0).float(), x.std(0, unbiased=self.nrep > 1).float()
+
+
+def C_stream(s: torch.cuda.Stream):
+    import ctypes
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _cache_file():
+    d = os.environ.get('NIPET_B200_CACHE', os.path.join(os.path.expanduser('~'), '.cache',
+                                                        'nipet_b200'))
+    return os.path.join(d, 'autotune.json')
+
+
+def autotune(rec: BatchRecon, candidates=None, repeats: int = 2) -> int:
+    """Pick the batch width (images per Siddon walk) with the best images/s for this
+    device, span and batch size, timing `repeats` sub-iterations per candidate.  Results
+    are cached in memory and in `~/.cache/nipet_b200/autotune.json`."""
+    name = torch.cuda.get_device_name(rec.device)
+    key = f'{name}|span{rec.span}|n{rec.nrep}'
+    if key in _TUNE_CACHE:
+        return _TUNE_CACHE[key]
+    try:
+        with open(_cache_file()) as f:
+            disk = json.load(f)
+        if key in disk:
+            _TUNE_CACHE[key] = int(disk[key])
+            return _TUNE_CACHE[key]
+    except Exception:
+        disk = {}
+    if candidates is None:
+        candidates = [1, 2, 4] if rec.span == 11 else [1, 2]
+    candidates = [c for c in candidates if c <= max(1, rec.nrep) or c == 1]
+    best, best_t = candidates[0], float('inf')
+    rec.sens128.fill_(1.0)
+    for bs in candidates:
+        rec.bs = bs
+        rec._alloc()
+        rec.init_images()
+        rec.subiteration(0)           # warm-up (also sets kernel attributes)
+        torch.cuda.synchronize(rec.device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            rec.subiteration(1)
+        e1.record()
+        torch.cuda.synchronize(rec.device)
+        t = e0.elapsed_time(e1)
+        if t < best_t:
+            best, best_t = bs, t
+    rec.geom.check()
+    _TUNE_CACHE[key] = best
+    try:
+        os.makedirs(os.path.dirname(_cache_file()), exist_ok=True)
+        disk[key] = best
+        with open(_cache_file(), 'w') as f:
+            json.dump(disk, f, indent=1)
+    except Exception:
+        pass
+    rec.bs = best
+    return best

@@ -1,0 +1,598 @@
+// nb_batch.cu -- OSEM for many images at once: bootstrap replicates or dynamic frames that
+// share the scanner geometry, attenuation, normalisation and sensitivity, each with its
+// own prompts and image (the batched configuration of the reference's osem(),
+// prj/src/recon.cu:318-497, run for all replicates in one launch per sub-iteration).
+//
+// Layout: "col128 x Bs" -- images grouped Bs at a time, group g at
+// img + g * [320*320][128][Bs]; inside a column the Bs replicate values of a voxel are
+// contiguous, so one 16-byte shared load (Bs = 4) feeds four replicates and every
+// geometric decision of the Siddon walk (crossing test, cursor update, segment lengths)
+// is shared by the Bs replicates of a ray.  A persistent CTA takes (LOR, group) jobs; per
+// job it runs the forward pass of the LOR for the Bs images, forms the Bs ratio rows
+// y_b / (Ax_b + c_b (r+s)/(an)) and back projects them, exactly as the single-image
+// kernel (nb_project.cuh) does for one image.
+#include <math.h>
+
+#include "nb_axial.cuh"
+#include "nb_internal.cuh"
+#include "nb_project.cuh"
+
+namespace nbb {
+
+using nbk::WAIT_POLLS;
+using nbk::lds_f32;
+using nbk::reds_add_s32;
+
+constexpr int NB_MAXREP = 1024;
+
+struct BatchArgs {
+  const int32_t *scol;
+  const float *st;
+  const float4 *hdr;
+  const nb_ray *rays;
+  const int16_t *bin11;
+  const int16_t *bin1;
+  const int32_t *subs;
+  int nprj, naw, span, ngroups, nrep;
+  const float *img;        // [ngroups][NCOL][128][Bs]
+  float *bimg;             // same layout, accumulated
+  const uint16_t *psng;    // [nrep][naw][nout]
+  const float *rs;         // [naw][nout] (r+s)/(an), scaled per replicate by rscale
+  const float *rscale;     // [nrep]
+  int fxbits;
+  int *err;
+};
+
+// shared-memory layout; every region starts on a 128-byte boundary (the mbarriers in the
+// misc region need 8-byte, the vector/TMA accesses 16-byte alignment)
+__host__ __device__ constexpr size_t align128(size_t x) { return (x + 127) & ~(size_t)127; }
+
+template <int BS, int CH> struct BSmem {
+  static constexpr size_t col_bytes = (size_t)NB_COLW * BS * sizeof(float);
+  static constexpr size_t buf_bytes = 2ull * CH * col_bytes;
+  static constexpr size_t fbuf_off = 0;
+  static constexpr size_t ibuf_off = align128(buf_bytes);
+  static constexpr size_t tn_off = align128(ibuf_off + buf_bytes);
+  static constexpr size_t vals_off = align128(tn_off + 2ull * CH * sizeof(float));
+  static constexpr size_t rat_off = align128(vals_off + 4096ull * BS * sizeof(float));
+  template <int NOUT> __host__ __device__ static constexpr size_t misc_off() {
+    return align128(rat_off + (size_t)NOUT * BS * sizeof(float));
+  }
+  template <int NOUT> __host__ __device__ static constexpr size_t total() {
+    return misc_off<NOUT>() + 64;
+  }
+};
+
+struct BJob {
+  int p, g, lor, n, nch, c, valid;
+};
+
+template <int CH>
+__device__ __forceinline__ void bjob_load(const BatchArgs &a, int q, BJob &J) {
+  J.valid = q < a.nprj * a.ngroups;
+  J.c = 0;
+  if (!J.valid) return;
+  J.p = q / a.ngroups;
+  J.g = q - J.p * a.ngroups;
+  const int lor = a.subs ? a.subs[J.p] : J.p;
+  if (lor < 0 || lor >= a.naw) {
+    if (threadIdx.x == 0) nb_set_error(a.err, NB_DEVERR_BAD_LOR);
+    J.lor = 0;
+    J.n = 0;
+  } else {
+    J.lor = lor;
+    J.n = __float_as_int(a.hdr[lor].w);
+  }
+  J.nch = J.n > 0 ? (J.n + CH - 1) / CH : 1;
+}
+
+template <int CH> __device__ __forceinline__ void bjob_next(const BatchArgs &a, BJob &J, int &q) {
+  if (++J.c >= 2 * J.nch) {
+    q += gridDim.x;
+    bjob_load<CH>(a, q, J);
+  }
+}
+
+template <int BS, int CH>
+__device__ __forceinline__ void bissue_load(const BatchArgs &a, const BJob &J, int chunk,
+                                            float *cols, float *tnb, uint64_t *bar) {
+  constexpr uint32_t colb = NB_COLW * BS * 4;
+  const int lane = threadIdx.x & 31;
+  const int s0 = chunk * CH;
+  const int n = max(0, min(CH, J.n - s0));
+  const uint32_t tn_bytes = max(16u, (uint32_t)((n * 4 + 15) & ~15));
+  if (lane == 0) nb_mbar_arrive_expect_tx(bar, (uint32_t)n * colb + tn_bytes);
+  __syncwarp();
+  const int32_t *sc = a.scol + (size_t)J.lor * NB_STEP_STRIDE + s0;
+  const float *gimg = a.img + (size_t)J.g * NB_NCOL * NB_COLW * BS;
+  for (int i = lane; i < n; i += 32)
+    nb_bulk_g2s(cols + (size_t)i * NB_COLW * BS, gimg + (size_t)sc[i] * NB_COLW * BS, colb, bar);
+  if (lane == 0) nb_bulk_g2s(tnb, a.st + (size_t)J.lor * NB_STEP_STRIDE + s0, tn_bytes, bar);
+}
+
+template <int CH>
+__device__ __forceinline__ void bload_tn(const BatchArgs &a, const BJob &J, int chunk, float *tnb) {
+  const int lane = threadIdx.x & 31;
+  const int s0 = chunk * CH;
+  const int n = max(0, min(CH, J.n - s0));
+  for (int i = lane; i < n; i += 32) tnb[i] = a.st[(size_t)J.lor * NB_STEP_STRIDE + s0 + i];
+}
+
+// rays of one thread: ray index = threadIdx.x + NT * r, r < RPT (NT * RPT >= 4084)
+template <int BS, int RPT> struct BRay {
+  float acc[RPT][BS];
+  float tzc[RPT], dtz[RPT];
+  int zo[RPT], dz4[RPT], dir4[RPT];  // byte offsets in units of 4*BS bytes per slot
+  float tp;
+};
+
+template <int BS, int NT, int RPT>
+__device__ __forceinline__ void brays_init(const BatchArgs &a, const float4 h, BRay<BS, RPT> &S) {
+  S.tp = h.x;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    const int ray = threadIdx.x + NT * r;
+#pragma unroll
+    for (int k = 0; k < BS; k++) S.acc[r][k] = 0.f;
+    if (ray < NB_NRAYS) {
+      nb_axial A;
+      nb_axial_setup(a.rays[ray], h.y, h.x, h.z, A);
+      S.zo[r] = 4 * BS * nb_zi(A.w);
+      S.tzc[r] = A.tzc;
+      S.dtz[r] = A.dtz;
+      S.dir4[r] = 4 * BS * A.dir;
+      S.dz4[r] = 4 * BS *
+                 (A.dir > 0 ? ((A.w & 1) ? -63 : 64) : (A.dir < 0 ? ((A.w & 1) ? -64 : 63) : 0));
+    } else {
+      S.zo[r] = 4 * BS * 127;
+      S.tzc[r] = __int_as_float(0x7f800000);
+      S.dtz[r] = 0.f;
+      S.dir4[r] = 0;
+      S.dz4[r] = 0;
+    }
+  }
+}
+
+// oblique length factor sqrt(1 + (dz/atn)^2) of a ray (1 for direct planes)
+__device__ __forceinline__ float oblique_s(const nb_ray &R, float atn) {
+  if (R.kind == 0) return 1.f;
+  const float az_atn = __fdiv_rn(__fsub_rn(R.r1z, R.r0z), atn);
+  return __fsqrt_rn(__fmaf_rn(az_atn, az_atn, 1.0f));
+}
+
+template <int BS> struct VecT;
+template <> struct VecT<1> { static __device__ __forceinline__ void ld(uint32_t a, float *v) { v[0] = lds_f32(a); } };
+template <> struct VecT<2> {
+  static __device__ __forceinline__ void ld(uint32_t a, float *v) {
+    asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(v[0]), "=f"(v[1]) : "r"(a));
+  }
+};
+template <> struct VecT<4> {
+  static __device__ __forceinline__ void ld(uint32_t a, float *v) {
+    asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+                 : "r"(a));
+  }
+};
+
+template <int BS, int RPT, bool BWD>
+__device__ __forceinline__ void bstep(BRay<BS, RPT> &S, int r, uint32_t &cur, float tn, float tp,
+                                      float lt, uint32_t off) {
+  if (!BWD) {
+    float v0[BS];
+    VecT<BS>::ld(cur + off, v0);
+#pragma unroll
+    for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(lt, v0[k], S.acc[r][k]);
+    if (tn > S.tzc[r]) {
+      cur += S.dz4[r];
+      S.dz4[r] = S.dir4[r] - S.dz4[r];
+      float v1[BS];
+      VecT<BS>::ld(cur + off, v1);
+      const float fb = __fsub_rn(tn, S.tzc[r]);
+#pragma unroll
+      for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(fb, v1[k] - v0[k], S.acc[r][k]);
+      S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
+    }
+  } else {
+    // backward accumulators are replicate-major inside a column ([BS][128] ints): the
+    // cursor is in units of 4 bytes per slot and replicate k adds k * 512 bytes, so the
+    // lanes of a warp (neighbouring slots) hit neighbouring banks
+    constexpr int LG = BS == 4 ? 2 : (BS == 2 ? 1 : 0);
+    if (tn > S.tzc[r]) {
+      const float fa = __fsub_rn(S.tzc[r], tp);
+#pragma unroll
+      for (int k = 0; k < BS; k++)
+        reds_add_s32(cur + off + 512u * k, __float2int_rn(fa * S.acc[r][k]));
+      cur += S.dz4[r] >> LG;
+      S.dz4[r] = S.dir4[r] - S.dz4[r];
+      const float fb = __fsub_rn(tn, S.tzc[r]);
+#pragma unroll
+      for (int k = 0; k < BS; k++)
+        reds_add_s32(cur + off + 512u * k, __float2int_rn(fb * S.acc[r][k]));
+      S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < BS; k++)
+        reds_add_s32(cur + off + 512u * k, __float2int_rn(lt * S.acc[r][k]));
+    }
+  }
+}
+
+template <int BS, int RPT, bool BWD>
+__device__ __forceinline__ void bwalk(BRay<BS, RPT> &S, const void *chunk, const float *tnb, int n) {
+  constexpr uint32_t colb = NB_COLW * BS * 4;
+  constexpr int LG = BWD ? (BS == 4 ? 2 : (BS == 2 ? 1 : 0)) : 0;  // see bstep
+  const uint32_t sb = nb_smem_u32(chunk);
+  uint32_t cur[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; r++) cur[r] = sb + (uint32_t)(S.zo[r] >> LG);
+  float tp = S.tp;
+  int i = 0;
+  for (; i + 4 <= n; i += 4) {
+    const float4 t4 = *reinterpret_cast<const float4 *>(tnb + i);
+    const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const float tn = tv[u];
+      const float lt = __fsub_rn(tn, tp);
+#pragma unroll
+      for (int r = 0; r < RPT; r++) bstep<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, u * colb);
+      tp = tn;
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; r++) cur[r] += 4 * colb;
+  }
+  for (; i < n; i++) {
+    const float tn = tnb[i];
+    const float lt = __fsub_rn(tn, tp);
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      bstep<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, 0u);
+      cur[r] += colb;
+    }
+    tp = tn;
+  }
+  S.tp = tp;
+#pragma unroll
+  for (int r = 0; r < RPT; r++) S.zo[r] = ((int)(cur[r] - sb) - n * (int)colb) << LG;
+}
+
+template <int BS, int CH, int NOUT, int NT, int RPT>
+__global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  using L = BSmem<BS, CH>;
+  constexpr int COLF = NB_COLW * BS;  // floats per column
+  float *fbuf = reinterpret_cast<float *>(smem_raw + L::fbuf_off);
+  int *ibuf = reinterpret_cast<int *>(smem_raw + L::ibuf_off);
+  float *tnbuf = reinterpret_cast<float *>(smem_raw + L::tn_off);
+  float *vals = reinterpret_cast<float *>(smem_raw + L::vals_off);   // [4096][BS]
+  float *rat = reinterpret_cast<float *>(smem_raw + L::rat_off);     // [NOUT][BS]
+  unsigned char *misc = smem_raw + L::template misc_off<NOUT>();
+  uint64_t *bars = reinterpret_cast<uint64_t *>(misc);
+  int *sflag = reinterpret_cast<int *>(misc + 16);
+  unsigned *smax = reinterpret_cast<unsigned *>(misc + 24);  // [2][BS] -> use [2] per lane set
+
+  const int tid = threadIdx.x;
+  const bool warp0 = tid < 32;
+  if (tid == 0) {
+    nb_mbar_init(&bars[0], 1);
+    nb_mbar_init(&bars[1], 1);
+    *sflag = 0;
+    smax[0] = 0u;
+    smax[1] = 0u;
+    nb_fence_mbar_init();
+  }
+  for (int i = tid; i < 2 * CH * COLF; i += NT) ibuf[i] = 0;
+  __syncthreads();
+
+  BJob J, P;
+  int qJ = blockIdx.x, qP = blockIdx.x;
+  bjob_load<CH>(a, qJ, J);
+  if (warp0) {
+    P = J;
+    for (int k = 0; k < 2 && P.valid; k++) {
+      const bool ld = P.c < P.nch;
+      const int chunk = ld ? P.c : P.c - P.nch;
+      if (ld)
+        bissue_load<BS, CH>(a, P, chunk, fbuf + (size_t)k * CH * COLF, tnbuf + k * CH, &bars[k]);
+      else
+        bload_tn<CH>(a, P, chunk, tnbuf + k * CH);
+      bjob_next<CH>(a, P, qP);
+    }
+  }
+  __syncthreads();
+
+  BRay<BS, RPT> S;
+  float inv_scale = 0.f;
+  uint32_t phase = 0;
+  int j = 0, nlor = 0;
+  while (J.valid) {
+    const int b = j & 1;
+    float *fb = fbuf + (size_t)b * CH * COLF;
+    int *ib = ibuf + (size_t)b * CH * COLF;
+    float *tb = tnbuf + b * CH;
+    const bool load = J.c < J.nch;
+    const int chunk = load ? J.c : J.c - J.nch;
+    const int n = max(0, min(CH, J.n - chunk * CH));
+    const float4 h = a.hdr[J.lor];
+
+    if (chunk == 0) {
+      brays_init<BS, NT, RPT>(a, h, S);
+      if (!load) {
+        float m = 0.f;
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+          const int ray = tid + NT * r;
+          float s = 0.f;
+          int o = 0;
+          if (ray < NB_NRAYS) {
+            const nb_ray R = a.rays[ray];
+            o = (NOUT == NB_NSN11) ? R.out11 : R.out1;
+            s = oblique_s(R, h.y);
+          }
+#pragma unroll
+          for (int k = 0; k < BS; k++) {
+            const float v = (ray < NB_NRAYS) ? rat[o * BS + k] * s : 0.f;
+            S.acc[r][k] = v;
+            m = fmaxf(m, fabsf(v));
+          }
+        }
+        for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const int par = nlor & 1;
+        if ((tid & 31) == 0 && m > 0.f) atomicMax(&smax[par], __float_as_uint(m));
+        __syncthreads();
+        const unsigned mb = smax[par];
+        if (tid == 0) smax[par ^ 1] = 0u;
+        float scale = 0.f;
+        inv_scale = 0.f;
+        if (mb != 0u && (mb >> 23) < 255u) {
+          const int e = (int)(mb >> 23) - 126;
+          scale = ldexpf(1.f, a.fxbits - e);
+          inv_scale = ldexpf(1.f, e - a.fxbits);
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+#pragma unroll
+          for (int k = 0; k < BS; k++) S.acc[r][k] *= scale;
+        ++nlor;
+      }
+    }
+
+    if (load) {
+      if (!nb_mbar_wait(&bars[b], (phase >> b) & 1u, WAIT_POLLS)) atomicExch(sflag, 1);
+      phase ^= 1u << b;
+      bwalk<BS, RPT, false>(S, fb, tb, n);
+    } else {
+      if (warp0) nb_bulk_wait_read<1>();
+      bwalk<BS, RPT, true>(S, ib, tb, n);
+      __syncthreads();
+      // int32 [col][BS][128] -> float staging [col][128][BS] (the image layout the bulk
+      // reduce adds into), zeroing the accumulators; slot 127 (padding) is not written back
+      const int nv = n * COLF;
+      for (int x = tid; x < nv; x += NT) {
+        const int c = x / COLF, rem = x - c * COLF;
+        const int slot = rem / BS, k = rem - slot * BS;
+        const int src = c * COLF + k * NB_COLW + slot;
+        const int q = ib[src];
+        fb[x] = slot == 127 ? 0.f : (float)q * inv_scale;
+        ib[src] = 0;
+      }
+      nb_fence_proxy_async_smem();
+    }
+
+    if (load && chunk == J.nch - 1) {
+#pragma unroll
+      for (int r = 0; r < RPT; r++) {
+        const int ray = tid + NT * r;
+        if (ray < NB_NRAYS) {
+          const float s = oblique_s(a.rays[ray], h.y);
+#pragma unroll
+          for (int k = 0; k < BS; k++) vals[ray * BS + k] = S.acc[r][k] * s;
+        }
+      }
+      __syncthreads();
+      for (int x = tid; x < NOUT * BS; x += NT) {
+        const int o = x / BS, k = x - o * BS;
+        float v;
+        if (NOUT == NB_NSN11) {
+          v = 0.f;
+          const int16_t *lst = a.bin11 + o * 8;
+#pragma unroll
+          for (int qq = 0; qq < 8; qq++) {
+            const int ray = lst[qq];
+            if (ray >= 0) v += vals[ray * BS + k];
+          }
+        } else {
+          v = vals[a.bin1[o] * BS + k];
+        }
+        const int rep = J.g * BS + k;
+        float rr = 0.f;
+        if (rep < a.nrep) {
+          const size_t gi = (size_t)J.lor * NOUT + o;
+          const float e = v + a.rscale[rep] * a.rs[gi];
+          const float y = (float)a.psng[(size_t)rep * a.naw * NOUT + gi];
+          rr = (e > -0.000001f && e < 0.000001f) ? 0.f : __fdiv_rn(y, e);
+        }
+        rat[x] = rr;
+      }
+    }
+
+    __syncthreads();
+    if (*sflag) break;
+
+    if (warp0) {
+      if (!load) {
+        const int32_t *sc = a.scol + (size_t)J.lor * NB_STEP_STRIDE + chunk * CH;
+        float *gb = a.bimg + (size_t)J.g * NB_NCOL * COLF;
+        for (int i = tid; i < n; i += 32)
+          nb_bulk_reduce_add_f32(gb + (size_t)sc[i] * COLF, fb + (size_t)i * COLF, COLF * 4);
+      }
+      nb_bulk_commit();
+      if (P.valid) {
+        const bool ld = P.c < P.nch;
+        const int pch = ld ? P.c : P.c - P.nch;
+        if (ld) {
+          nb_bulk_wait_read<0>();
+          bissue_load<BS, CH>(a, P, pch, fb, tb, &bars[b]);
+        } else {
+          bload_tn<CH>(a, P, pch, tb);
+        }
+        bjob_next<CH>(a, P, qP);
+      }
+    }
+    bjob_next<CH>(a, J, qJ);
+    ++j;
+  }
+  if (*sflag && tid == 0) nb_set_error(a.err, NB_DEVERR_MBAR_TIMEOUT);
+  if (warp0) nb_bulk_wait_all<0>();
+}
+
+}  // namespace nbb
+
+// ---------------------------------------------------------------------------------------
+// layout conversion and the batched image update
+// ---------------------------------------------------------------------------------------
+namespace {
+
+// [nrep][320*320][127] (reference layout) <-> [ngroups][320*320][128][BS]
+__global__ void k_to_batch(float *__restrict__ dst, const float *__restrict__ src, int nrep,
+                           int bs) {
+  const size_t n = (size_t)nrep * NB_NCOL * NB_COLW;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(t % NB_COLW);
+    const size_t rc = t / NB_COLW;
+    const int col = (int)(rc % NB_NCOL);
+    const int rep = (int)(rc / NB_NCOL);
+    const int g = rep / bs, k = rep - g * bs;
+    const float v = z < NB_IMZ ? src[((size_t)rep * NB_NCOL + col) * NB_IMZ + z] : 0.f;
+    dst[(((size_t)g * NB_NCOL + col) * NB_COLW + nb_zi(z)) * bs + k] = v;
+  }
+}
+
+__global__ void k_from_batch(float *__restrict__ dst, const float *__restrict__ src, int nrep,
+                             int bs) {
+  const size_t n = (size_t)nrep * NB_NCOL * NB_IMZ;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(t % NB_IMZ);
+    const size_t rc = t / NB_IMZ;
+    const int col = (int)(rc % NB_NCOL);
+    const int rep = (int)(rc / NB_NCOL);
+    const int g = rep / bs, k = rep - g * bs;
+    dst[t] = src[(((size_t)g * NB_NCOL + col) * NB_COLW + nb_zi(z)) * bs + k];
+  }
+}
+
+// img = msk ? img * (|sens| < 1e-6 ? 0 : bimg / sens) : 0; bimg = 0  (recon.cu:493-496),
+// sens and msk shared by the BS images of a group
+__global__ void k_update_batch(float *__restrict__ img, float *__restrict__ bimg,
+                               const float *__restrict__ sens, const uint8_t *__restrict__ msk,
+                               int ngroups, int bs) {
+  const size_t nvox = (size_t)NB_NCOL * NB_COLW;
+  const size_t n = (size_t)ngroups * nvox * bs;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t v = (t / bs) % nvox;
+    const float s = sens[v];
+    const float q = (s > -0.000001f && s < 0.000001f) ? 0.f : __fdiv_rn(bimg[t], s);
+    img[t] = msk[v] ? img[t] * q : 0.f;
+    bimg[t] = 0.f;
+  }
+}
+
+template <int BS, int CH, int NOUT, int NT, int RPT>
+int launch_batch(nb_geom *g, const nbb::BatchArgs &a, cudaStream_t s) {
+  static_assert(NT * RPT >= NB_NRAYS, "not enough ray slots");
+  static_assert(nbb::BSmem<BS, CH>::template misc_off<NOUT>() % 128 == 0, "misaligned barriers");
+  static_assert(nbb::BSmem<BS, CH>::template total<NOUT>() <= 227 * 1024, "too much shared memory");
+  const size_t smem = nbb::BSmem<BS, CH>::template total<NOUT>();
+  static bool set[64] = {false};
+  if (!set[g->device & 63]) {
+    NB_CUDA(cudaFuncSetAttribute(nbb::k_osem_batch<BS, CH, NOUT, NT, RPT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set[g->device & 63] = true;
+  }
+  const long jobs = (long)a.nprj * a.ngroups;
+  const int grid = jobs < g->nsm ? (int)jobs : g->nsm;
+  if (grid <= 0) return NB_OK;
+  nbb::k_osem_batch<BS, CH, NOUT, NT, RPT><<<grid, NT, smem, s>>>(a);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+}  // namespace
+
+extern "C" int nb_to_batch(float *dst, const float *src, int nrep, int bs, void *stream) {
+  NB_REQUIRE(dst && src && nrep > 0 && (bs == 1 || bs == 2 || bs == 4),
+             "nb_to_batch: bad arguments");
+  NB_CUDA(cudaMemsetAsync(dst, 0,
+                          sizeof(float) * (size_t)((nrep + bs - 1) / bs) * bs * NB_NCOL * NB_COLW,
+                          (cudaStream_t)stream));
+  k_to_batch<<<4096, 256, 0, (cudaStream_t)stream>>>(dst, src, nrep, bs);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+extern "C" int nb_from_batch(float *dst, const float *src, int nrep, int bs, void *stream) {
+  NB_REQUIRE(dst && src && nrep > 0 && (bs == 1 || bs == 2 || bs == 4),
+             "nb_from_batch: bad arguments");
+  k_from_batch<<<4096, 256, 0, (cudaStream_t)stream>>>(dst, src, nrep, bs);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens128,
+                                    const uint8_t *msk128, const uint16_t *psng, const float *rs,
+                                    const float *rscale, int nrep, int bs, int span,
+                                    const int32_t *subs, int nprj, void *stream) {
+  NB_REQUIRE(g != nullptr, "nb_osem_batch_subset: NULL geometry handle");
+  NB_REQUIRE(img && bimg && sens128 && msk128 && psng && rs && rscale && subs,
+             "nb_osem_batch_subset: NULL argument");
+  NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_osem_batch_subset: nrep out of range");
+  NB_REQUIRE(span == 11 || span == 1, "nb_osem_batch_subset: span must be 1 or 11");
+  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
+             "nb_osem_batch_subset: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(nprj > 0, "nb_osem_batch_subset: empty subset");
+  NB_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ngroups = (nrep + bs - 1) / bs;
+  nbb::BatchArgs a{};
+  a.scol = g->d_scol;
+  a.st = g->d_st;
+  a.hdr = g->d_hdr;
+  a.rays = g->d_rays;
+  a.bin11 = g->d_bin11;
+  a.bin1 = g->d_bin1;
+  a.subs = subs;
+  a.nprj = nprj;
+  a.naw = g->naw;
+  a.span = span;
+  a.ngroups = ngroups;
+  a.nrep = nrep;
+  a.img = img;
+  a.bimg = bimg;
+  a.psng = psng;
+  a.rs = rs;
+  a.rscale = rscale;
+  a.fxbits = g->fxbits;
+  a.err = g->d_err;
+  int st;
+  if (span == 11) {
+    if (bs == 4)
+      st = launch_batch<4, 16, NB_NSN11, 512, 8>(g, a, s);
+    else if (bs == 2)
+      st = launch_batch<2, 32, NB_NSN11, 512, 8>(g, a, s);
+    else
+      st = launch_batch<1, 64, NB_NSN11, 1024, 4>(g, a, s);
+  } else {
+    if (bs == 2)
+      st = launch_batch<2, 32, NB_NSN1, 512, 8>(g, a, s);
+    else
+      st = launch_batch<1, 64, NB_NSN1, 1024, 4>(g, a, s);
+  }
+  if (st) return st;
+  k_update_batch<<<g->nsm * 16, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups, bs);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}

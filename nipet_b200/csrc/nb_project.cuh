@@ -62,6 +62,7 @@ struct PrjArgs {
 };
 
 template <int MODE, int CH> struct Smem {
+  static_assert((2ull * CH * sizeof(float)) % 128 == 0, "tn buffers must keep 128-byte alignment");
   static constexpr bool HAS_I = MODE != MODE_FWD;
   static constexpr size_t buf_bytes = 2ull * CH * NB_COLW * sizeof(float);
   static constexpr size_t fbuf_off = 0;                 // forward columns / backward staging
@@ -71,6 +72,8 @@ template <int MODE, int CH> struct Smem {
   static constexpr size_t rat_off = vals_off + 4096 * sizeof(float);
   static constexpr size_t misc_off = rat_off + (MODE == MODE_OSEM ? 4096 * sizeof(float) : 0);
   static constexpr size_t total = misc_off + 64;
+  static_assert(misc_off % 128 == 0, "mbarriers must be aligned");
+  static_assert(total <= 227 * 1024, "too much shared memory");
 };
 
 struct Job {

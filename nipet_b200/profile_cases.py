@@ -12,6 +12,10 @@ launches 15, 16, 17 are one warm launch of each mode:
         python -m nipet_b200.profile_cases projectors
 
 `hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2).
+
+`batch` runs one batched OSEM sub-iteration (subset 0) for 8 images with batch widths 4 and
+2, twice each (capture -k regex:k_osem_batch -s 2 -c 2 for the second launch of each width:
+launches 0, 1 are width 4, 2, 3 width 2 -- use -s 1 -c 1 and -s 3 -c 1).
 """
 from __future__ import annotations
 
@@ -66,5 +70,28 @@ def hist(device='cuda:0'):
     print('hist ok', int(r['phc'].sum()))
 
 
+def batch(device='cuda:0'):
+    from . import batch as B
+    from . import geometry
+    dev = torch.device(device)
+    p = geometry.get_mmrparams()
+    gen = torch.Generator(device=dev).manual_seed(0)
+    nrep = 8
+    y = torch.randint(0, 6, (nrep, 68516, 837), device=dev, generator=gen).to(torch.int32).to(
+        torch.uint16)
+    an = torch.rand((68516, 837), device=dev, generator=gen) + 0.5
+    rs = torch.full((68516, 837), 0.01, device=dev)
+    for bs in (4, 2):
+        br = B.BatchRecon(p, y, rs, an, device=dev, bs=bs)
+        br.sens128.fill_(1.0)
+        br.init_images()
+        for _ in range(2):
+            br.subiteration(0)
+        torch.cuda.synchronize(dev)
+        br.geom.check()
+        del br
+    print('batch ok')
+
+
 if __name__ == '__main__':
-    {'projectors': projectors, 'hist': hist}[sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
+    {'projectors': projectors, 'hist': hist, 'batch': batch}[sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
