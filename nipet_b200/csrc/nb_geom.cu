@@ -304,6 +304,31 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
     }
     rays[r] = R;
   }
+  // Warp-friendly ray order: the kernels give thread t the rays t, t+NT, ... so every
+  // 32-aligned block of ray indices is the lane set of one warp.  Rays of one ring
+  // difference and direction (a "group") sit 2 voxels apart and cross z planes at the same
+  // steps; a warp drawn from one group reads consecutive shared-memory banks and takes
+  // its crossings together.  So each group's full blocks of 32 come first, and the group
+  // remainders (fewer than 32 rays each) are packed after them.
+  {
+    const std::vector<nb_ray> canon = rays;
+    std::vector<int> order, rest;
+    order.reserve(NB_NRAYS);
+    int start = 0;
+    auto key = [&](int r) {
+      return canon[r].kind * 1000 + (int)lrintf((canon[r].r1z - canon[r].r0z) / NB_RING);
+    };
+    for (int r = 1; r <= NB_NRAYS; r++) {
+      if (r == NB_NRAYS || key(r) != key(start)) {
+        const int len = r - start, full = len / 32 * 32;
+        for (int i = 0; i < full; i++) order.push_back(start + i);
+        for (int i = full; i < len; i++) rest.push_back(start + i);
+        start = r;
+      }
+    }
+    order.insert(order.end(), rest.begin(), rest.end());
+    for (int r = 0; r < NB_NRAYS; r++) rays[r] = canon[order[r]];
+  }
   std::vector<int16_t> bin11(NB_NSN11 * 8, -1), bin1(NB_NSN1, -1);
   std::vector<int> cnt11(NB_NSN11, 0);
   for (int r = 0; r < NB_NRAYS; r++) {

@@ -67,7 +67,7 @@ __global__ void k_osem_update(float4 *__restrict__ img, float4 *__restrict__ bim
   }
 }
 
-// V: voxel reads of a full forward projection, one thread per (LOR, oblique pair)
+// V: voxel reads of a full forward projection, one block per LOR
 __global__ void k_count_reads(const float4 *__restrict__ hdr, const float *__restrict__ st,
                               const nb_ray *__restrict__ rays, int naw,
                               unsigned long long *out, unsigned long long *per_lor) {
@@ -75,21 +75,22 @@ __global__ void k_count_reads(const float4 *__restrict__ hdr, const float *__res
   if (lor >= naw) return;
   const float4 h = hdr[lor];
   const int n = __float_as_int(h.w);
+  // per ray: one read per step, one more at each axial crossing (a +RD/-RD pair of the
+  // reference: 2 per step, 4 at a crossing); direct rays never cross
   unsigned long long tot = 0;
-  for (int li = NB_NRINGS + threadIdx.x; li < NB_NLI2R; li += blockDim.x) {
+  for (int ray = threadIdx.x; ray < NB_NRAYS; ray += blockDim.x) {
     nb_axial A;
-    nb_axial_setup(rays[li], h.y, h.x, h.z, A);
+    nb_axial_setup(rays[ray], h.y, h.x, h.z, A);
     float tzc = A.tzc;
+    tot += n;
     for (int k = 0; k < n; k++) {
-      float tn = st[(size_t)lor * NB_STEP_STRIDE + k];
-      if (__fsub_rn(tn, tzc) > 0.f) {
-        tot += 4;
+      const float tn = st[(size_t)lor * NB_STEP_STRIDE + k];
+      if (tn > tzc) {
+        tot += 1;
         tzc = __fadd_rn(tzc, A.dtz);
-      } else
-        tot += 2;
+      }
     }
   }
-  if (threadIdx.x == 0) tot += (unsigned long long)NB_NRINGS * n;
   atomicAdd(out, tot);
   atomicAdd(per_lor + lor, tot);
 }
