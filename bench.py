@@ -1,20 +1,26 @@
 """Benchmark of the mMR reconstruction hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload osem|hist]
+                    [--workload batch|osem|hist] [--replicates R]
 
 Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand in for):
-  osem  one full OSEM reconstruction per step: 14 sensitivity images + 4 iterations x 14
-        subsets, span-11 (837 x 252 x 344 sinograms), 320x320x127 float32 image, prompts
-        from a brain phantom with water attenuation, log-normal crystal efficiencies and
-        20% uniform randoms at 3e7 counts.  Metric: reconstructions per second.
+  batch (default) batched bootstrap OSEM: R = 50 Poisson replicates of one synthetic scan
+        (45 at 3e7 counts, 5 at 3e6), all reconstructed together per step: 14 sensitivity
+        images + 4 iterations x 14 subsets, span-11 (837 x 252 x 344 sinograms),
+        320x320x127 float32 images, one persistent launch per sub-iteration and one CUDA
+        graph per iteration.  Metric: reconstructions (replicates) per second.
+  osem  one plain OSEM reconstruction per step (same scan: brain phantom, water
+        attenuation, log-normal crystal efficiencies, 20% uniform randoms, 3e7 counts).
   hist  list-mode histogramming of a synthetic 32-bit mMR event stream (events/s).
 
 `value` is measured on device-resident inputs (CUDA events, barrier + synchronize on
-both sides, L2 flushed between steps); `e2e` times the public drop-in API
-(`petprj.bprj` / `petprj.osem` with host numpy arrays, host<->device copies inside the
-timed region).  Under torchrun (N > 1) every rank reconstructs its own scan (replicas,
-weak scaling) and the slowest rank's time is reported.
+both sides; inputs larger than L2, or L2 flushed between steps); `e2e` times the public
+API with host arrays and host<->device copies inside the timed region (`batch`:
+BatchRecon from pinned host prompts to host mean/std images; `osem`: `petprj.bprj` /
+`petprj.osem` with host numpy arrays).  `batch` also reports the plain drop-in
+(`petprj`, one replicate at a time) measured in the same run.  Under torchrun (N > 1)
+every rank reconstructs its own replicates (weak scaling) and the slowest rank's time
+is reported.
 """
 from __future__ import annotations
 
@@ -34,7 +40,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 NAW, NSN11 = 68516, 837
-METRIC = {'osem': ('OSEM recon/s span-11 320x320x127', 'recon/s'),
+METRIC = {'batch': ('OSEM recon/s span-11 320\u00b2\u00d7127 (batched+autograd vs plain), '
+                    'HBM GB/s vs peak', 'recon/s'),
+          'osem': ('OSEM recon/s span-11 320x320x127 (plain, one scan)', 'recon/s'),
           'hist': ('list-mode histogram events/s', 'events/s')}
 
 
@@ -250,23 +258,7 @@ def run_osem(args, ws, rank, dev):
     # e2e through the public drop-in API with host arrays (reference call pattern)
     e2e = None
     if args.e2e_steps > 0:
-        host = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
-        an = host['asng'] * host['nsng']
-        tab = mmrrec.subset_table(params)
-        msk = geometry.get_cylinder(Cnt, rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
-        krnl = np.full((3, 17), -1, np.float32)
-        sens = np.zeros((14, 320, 320, 127), np.float32)
-
-        def e2e_step():
-            for n in range(14):
-                rows = tab[n, 1:]
-                petprj.bprj(sens[n], an[rows], params['txLUT'], params['axLUT'], rows, Cnt)
-            img = np.ones((320, 320, 127), np.float32)
-            for _ in range(4):
-                petprj.osem(img, host['psng'], host['rsng'], host['ssng'], host['nsng'],
-                            host['asng'], tab, sens, msk, krnl, params['txLUT'],
-                            params['axLUT'], Cnt)
-            return img
+        e2e_step, host, an, tab, msk, sens = _plain_dropin(params, scan, dev, Cnt)
         e2e_step()
         et = []
         for _ in range(args.e2e_steps):
@@ -297,6 +289,167 @@ def run_osem(args, ws, rank, dev):
                                '4 it x 14 subsets + sensitivity, 3e7 counts',
                    'global_batch': ws, 'parallelism': f'replicas x{ws}',
                    'l2': 'flushed between steps (256 MB write)'},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        res['cpu_baseline'] = cpu_osem_sample(params)
+    return res
+
+
+# ---------------------------------------------------------------------------------------
+# batched bootstrap OSEM workload
+# ---------------------------------------------------------------------------------------
+def _plain_dropin(params, scan, dev, Cnt):
+    """One reconstruction through the plain drop-in API (`petprj.bprj` x14 for the
+    sensitivity images, `petprj.osem` x4 with host numpy arrays): returns (seconds, h2d, d2h)."""
+    import torch
+    from nipet_b200 import geometry, mmrrec, petprj
+    host = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
+    an = host['asng'] * host['nsng']
+    tab = mmrrec.subset_table(params)
+    msk = geometry.get_cylinder(Cnt, rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
+    krnl = np.full((3, 17), -1, np.float32)
+    sens = np.zeros((14, 320, 320, 127), np.float32)
+
+    def recon():
+        for n in range(14):
+            rows = tab[n, 1:]
+            petprj.bprj(sens[n], an[rows], params['txLUT'], params['axLUT'], rows, Cnt)
+        img = np.ones((320, 320, 127), np.float32)
+        for _ in range(4):
+            petprj.osem(img, host['psng'], host['rsng'], host['ssng'], host['nsng'],
+                        host['asng'], tab, sens, msk, krnl, params['txLUT'], params['axLUT'],
+                        Cnt)
+        return img
+    return recon, host, an, tab, msk, sens
+
+
+def run_batch(args, ws, rank, dev):
+    import torch
+    from nipet_b200 import batch, geometry, mmrrec
+
+    params = geometry.get_mmrparams()
+    Cnt = dict(params['Cnt'], DEVID=dev.index)
+    scan = mmrrec.synthetic_scan(params, dev, seed=rank)
+    nrep = args.replicates
+    nlow = max(0, min(nrep, round(nrep / 10)))
+    totals = [3e7] * (nrep - nlow) + [3e6] * nlow
+    rscale = [t / 3e7 for t in totals]
+    psng = batch.bootstrap_prompts(scan['mean'], totals, seed=1000 + rank)
+    an = (scan['asng'] * scan['nsng']).contiguous()
+    rs = torch.where(an.abs() < 1e-6, torch.zeros_like(an), scan['rsng'] / an)
+    br = batch.BatchRecon(params, psng, rs, an, rscale=rscale, device=dev)
+
+    def step():
+        br.sensitivity()
+        br.init_images()
+        for _ in range(4):
+            br.iteration(use_graph=True)
+
+    # per-launch algorithmic bytes of k_osem_batch (subset i): 8 B per forward voxel read and
+    # back-projection update per image, the images' prompt rows (2 B) and one (r+s)/(an)
+    # and a*n row per image group (4 B each)
+    _, per_lor = br.geom.count_reads(per_lor=True)
+    ngroups = (nrep + br.bs - 1) // br.bs
+    bytes_sub = [nrep * 8 * int(per_lor[s.cpu().numpy()].sum()) +
+                 br.nprj * NSN11 * (2 * nrep + 8 * ngroups) for s in br.subs]
+    bytes_iter = float(sum(bytes_sub))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    br.geom.check()
+    br.launches = 0
+    clk = Clocks(dev.index) if rank == 0 else None
+    times, it_ms = [], []
+    for _ in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        br.sensitivity()
+        br.init_images()
+        ev = []
+        for _ in range(4):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            br.iteration(use_graph=True)
+            e1.record()
+            ev.append((e0, e1))
+        t1.record()
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+        it_ms += [a.elapsed_time(b) for a, b in ev]
+    clocks = clk.stop() if clk else None
+    br.geom.check()
+    launches_per_step = br.launches // args.steps
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    value = ws * nrep / t_step
+    # roofline: one graph replay = 14 k_osem_batch launches + 14 image updates (the update
+    # kernels are ~1% of the replay); achieved = algorithmic bytes of the 14 launches / time
+    t_it = float(np.mean(it_ms)) / 1e3
+    achieved = bytes_iter / t_it / 1e9
+    peak, peak_kind = _peaks()
+    tr8 = _traffic('osem_batch_8img')
+    traffic = None if tr8 is None else tr8 * nrep / 8.0
+
+    # e2e through the public batch API: pinned host prompts -> device, reconstruction,
+    # voxel-wise mean/std images back to the host
+    host_psng = psng.cpu().pin_memory()
+    host_rs, host_an = rs.cpu().pin_memory(), an.cpu().pin_memory()
+    del psng
+    et = []
+    for _ in range(max(1, args.e2e_steps)):
+        _barrier(ws, dev)
+        t = time.perf_counter()
+        r2 = batch.BatchRecon(params, host_psng.to(dev, non_blocking=True),
+                              host_rs.to(dev, non_blocking=True),
+                              host_an.to(dev, non_blocking=True), rscale=rscale, device=dev,
+                              bs=br.bs)
+        r2.run(niter=4, use_graph=False)
+        m, s = r2.mean_std()
+        m, s = m.cpu(), s.cpu()
+        torch.cuda.synchronize(dev)
+        et.append(time.perf_counter() - t)
+        del r2
+    te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    h2d = host_psng.numel() * 2 + host_rs.numel() * 4 + host_an.numel() * 4
+    d2h = 2 * 320 * 320 * 127 * 4
+    e2e = {'value': ws * nrep / te, 'unit': 'recon/s', 'h2d_bytes_per_step': int(h2d),
+           'd2h_bytes_per_step': int(d2h),
+           'path': 'batch.BatchRecon(host prompts) -> run(4) -> mean_std() -> host'}
+
+    # the plain drop-in run sequentially (one replicate), for the batched/plain ratio
+    plain = None
+    if args.plain_steps > 0:
+        recon, *_ = _plain_dropin(params, scan, dev, Cnt)
+        recon()
+        pt = []
+        for _ in range(args.plain_steps):
+            t = time.perf_counter()
+            recon()
+            torch.cuda.synchronize(dev)
+            pt.append(time.perf_counter() - t)
+        tp = float(np.mean(pt))
+        plain = {'value': 1.0 / tp, 'unit': 'recon/s',
+                 'path': 'petprj.bprj x14 + petprj.osem x4, host numpy arrays, one replicate',
+                 'batched_e2e_over_plain': (nrep / te) / (1.0 / tp)}
+
+    res = {
+        'ms_per_step': t_step * 1e3, 'value': value, 'e2e': e2e, 'clocks': clocks,
+        'gpu_launches': launches_per_step, 'plain_dropin': plain,
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                     'frac': achieved / peak, 'traffic': traffic,
+                     'kernel': f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk)',
+                     'peak_kind': peak_kind, 'bytes_per_launch_avg': bytes_iter / len(br.subs),
+                     'launch_ms_avg': t_it * 1e3 / len(br.subs)},
+        'config': {'workload': f'batched bootstrap OSEM, {nrep} replicates '
+                               f'({nrep - nlow} at 3e7, {nlow} at 3e6 counts), span-11 '
+                               f'837x252x344, 320x320x127 f32, 4 it x 14 subsets + '
+                               f'sensitivity, CUDA graph per iteration',
+                   'global_batch': ws * nrep, 'batch_width': br.bs,
+                   'parallelism': f'replicas x{ws}', 'l2': 'inputs larger than L2 '
+                   f'({nrep} prompt sinograms, {nrep} images)'},
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         res['cpu_baseline'] = cpu_osem_sample(params)
@@ -368,7 +521,7 @@ def run_reference(args):
     params = geometry.get_mmrparams()
     metric, unit = METRIC[args.workload]
     vals = []
-    if args.workload == 'osem':
+    if args.workload in ('osem', 'batch'):
         for _ in range(args.warmup + args.steps):
             vals.append(cpu_osem_sample(params, seconds=6.0))
     else:
@@ -395,7 +548,9 @@ def main():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='osem', choices=['osem', 'hist'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'osem', 'hist'])
+    ap.add_argument('--replicates', type=int, default=50)
+    ap.add_argument('--plain-steps', type=int, default=1)
     ap.add_argument('--e2e-steps', type=int, default=1)
     ap.add_argument('--events', type=int, default=200_000_000)
     ap.add_argument('--duration', type=int, default=600)
@@ -412,17 +567,19 @@ def main():
     ws, rank, local = _dist()
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    res = run_osem(args, ws, rank, dev) if args.workload == 'osem' else run_hist(args, ws, rank,
-                                                                                  dev)
+    run = {'batch': run_batch, 'osem': run_osem, 'hist': run_hist}[args.workload]
+    res = run(args, ws, rank, dev)
     metric, unit = METRIC[args.workload]
     if rank == 0:
         line = {'metric': metric, 'value': res['value'], 'unit': unit, 'n_gpus': ws,
                 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms_per_step'],
                 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-                'dtype': 'f32' if args.workload == 'osem' else 'u32', 'data': 'synthetic',
+                'dtype': 'u32' if args.workload == 'hist' else 'f32', 'data': 'synthetic',
                 'config': res['config'], 'roofline': res['roofline'],
                 'cpu_baseline': res.get('cpu_baseline'), 'e2e': res['e2e'],
                 'gpu_launches': res['gpu_launches'], 'clocks': res['clocks']}
+        if res.get('plain_dropin') is not None:
+            line['plain_dropin'] = res['plain_dropin']
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
