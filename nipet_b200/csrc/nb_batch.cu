@@ -175,53 +175,57 @@ template <> struct VecT<4> {
   }
 };
 
+// One column step of ray r, split in two phases so that the rays of a thread run as
+// straight-line code: phase 1 (every ray) covers the segment in the current z slot -- the
+// whole column, or up to the z crossing -- and phase 2 (only the rays whose z crossing
+// falls inside this column) moves the cursor and covers the rest in the new slot.
+//   forward:  (tzc - tp) v0 + (tn - tzc) v1   on a crossing, lt v0 otherwise
+//   backward: the same weights times the ray's ratio, added to the two voxels
 template <int BS, int RPT, bool BWD>
-__device__ __forceinline__ void bstep(BRay<BS, RPT> &S, int r, uint32_t &cur, float tn, float tp,
-                                      float lt, uint32_t off) {
+__device__ __forceinline__ void bstep1(BRay<BS, RPT> &S, int r, uint32_t cur, float tn, float tp,
+                                       float lt, uint32_t off) {
+  const float w = (tn > S.tzc[r]) ? __fsub_rn(S.tzc[r], tp) : lt;
   if (!BWD) {
     float v0[BS];
     VecT<BS>::ld(cur + off, v0);
 #pragma unroll
-    for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(lt, v0[k], S.acc[r][k]);
-    if (tn > S.tzc[r]) {
-      cur += S.dz4[r];
-      S.dz4[r] = S.dir4[r] - S.dz4[r];
-      float v1[BS];
-      VecT<BS>::ld(cur + off, v1);
-      const float fb = __fsub_rn(tn, S.tzc[r]);
-#pragma unroll
-      for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(fb, v1[k] - v0[k], S.acc[r][k]);
-      S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
-    }
+    for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(w, v0[k], S.acc[r][k]);
   } else {
     // backward accumulators are replicate-major inside a column ([BS][128] ints): the
     // cursor is in units of 4 bytes per slot and replicate k adds k * 512 bytes, so the
     // lanes of a warp (neighbouring slots) hit neighbouring banks
-    constexpr int LG = BS == 4 ? 2 : (BS == 2 ? 1 : 0);
-    if (tn > S.tzc[r]) {
-      const float fa = __fsub_rn(S.tzc[r], tp);
 #pragma unroll
-      for (int k = 0; k < BS; k++)
-        reds_add_s32(cur + off + 512u * k, __float2int_rn(fa * S.acc[r][k]));
-      cur += S.dz4[r] >> LG;
-      S.dz4[r] = S.dir4[r] - S.dz4[r];
-      const float fb = __fsub_rn(tn, S.tzc[r]);
+    for (int k = 0; k < BS; k++)
+      reds_add_s32(cur + off + 512u * k, __float2int_rn(w * S.acc[r][k]));
+  }
+}
+
+template <int BS, int RPT, bool BWD>
+__device__ __forceinline__ void bstep2(BRay<BS, RPT> &S, int r, uint32_t &cur, float tn,
+                                       uint32_t off) {
+  if (tn > S.tzc[r]) {
+    constexpr int LG = BWD ? (BS == 4 ? 2 : (BS == 2 ? 1 : 0)) : 0;
+    cur += S.dz4[r] >> LG;
+    S.dz4[r] = S.dir4[r] - S.dz4[r];
+    const float fb = __fsub_rn(tn, S.tzc[r]);
+    if (!BWD) {
+      float v1[BS];
+      VecT<BS>::ld(cur + off, v1);
 #pragma unroll
-      for (int k = 0; k < BS; k++)
-        reds_add_s32(cur + off + 512u * k, __float2int_rn(fb * S.acc[r][k]));
-      S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
+      for (int k = 0; k < BS; k++) S.acc[r][k] = fmaf(fb, v1[k], S.acc[r][k]);
     } else {
 #pragma unroll
       for (int k = 0; k < BS; k++)
-        reds_add_s32(cur + off + 512u * k, __float2int_rn(lt * S.acc[r][k]));
+        reds_add_s32(cur + off + 512u * k, __float2int_rn(fb * S.acc[r][k]));
     }
+    S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
   }
 }
 
 template <int BS, int RPT, bool BWD>
 __device__ __forceinline__ void bwalk(BRay<BS, RPT> &S, const void *chunk, const float *tnb, int n) {
   constexpr uint32_t colb = NB_COLW * BS * 4;
-  constexpr int LG = BWD ? (BS == 4 ? 2 : (BS == 2 ? 1 : 0)) : 0;  // see bstep
+  constexpr int LG = BWD ? (BS == 4 ? 2 : (BS == 2 ? 1 : 0)) : 0;  // see bstep1
   const uint32_t sb = nb_smem_u32(chunk);
   uint32_t cur[RPT];
 #pragma unroll
@@ -236,7 +240,9 @@ __device__ __forceinline__ void bwalk(BRay<BS, RPT> &S, const void *chunk, const
       const float tn = tv[u];
       const float lt = __fsub_rn(tn, tp);
 #pragma unroll
-      for (int r = 0; r < RPT; r++) bstep<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, u * colb);
+      for (int r = 0; r < RPT; r++) bstep1<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, u * colb);
+#pragma unroll
+      for (int r = 0; r < RPT; r++) bstep2<BS, RPT, BWD>(S, r, cur[r], tn, u * colb);
       tp = tn;
     }
 #pragma unroll
@@ -246,8 +252,10 @@ __device__ __forceinline__ void bwalk(BRay<BS, RPT> &S, const void *chunk, const
     const float tn = tnb[i];
     const float lt = __fsub_rn(tn, tp);
 #pragma unroll
+    for (int r = 0; r < RPT; r++) bstep1<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, 0u);
+#pragma unroll
     for (int r = 0; r < RPT; r++) {
-      bstep<BS, RPT, BWD>(S, r, cur[r], tn, tp, lt, 0u);
+      bstep2<BS, RPT, BWD>(S, r, cur[r], tn, 0u);
       cur[r] += colb;
     }
     tp = tn;
