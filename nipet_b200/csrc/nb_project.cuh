@@ -196,11 +196,13 @@ static __device__ __forceinline__ void reds_add_s32(uint32_t addr, int v) {
   asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
-// One step of a ray, forward (prjf.cu:76-86 / :164-190).  The step covers [tp, tn]; a ray
-// that crosses a z plane at tzc inside it (at most one per step, as in the reference)
-// integrates [tp, tzc] in its current voxel v0 and [tzc, tn] in the next voxel v1, i.e.
-// lt*v0 + (tn - tzc)*(v1 - v0).  `cur` is the ray's shared-memory cursor: the address of
-// its voxel in the chunk's first column; step u of the chunk adds u*512 bytes.
+// One step of a ray covers [tp, tn] (prjf.cu:76-86 / :164-190 forward, prjb.cu:70-77 /
+// :153-178 backward).  A ray that crosses a z plane at tzc inside the step (at most one per
+// step, as in the reference) spends [tp, tzc] in its current voxel v0 and [tzc, tn] in the
+// next voxel v1.  `cur` is the ray's shared-memory cursor: the address of its voxel in the
+// chunk's first column; step u of the chunk adds u*512 bytes.
+//
+// Forward: lt*v0 + (tn - tzc)*(v1 - v0), one step per call.
 static __device__ __forceinline__ void step_fwd(float &acc, uint32_t &cur, int &dz4, float &tzc,
                                                 const int dir4, const float dtz, float tn, float lt,
                                                 uint32_t off) {
@@ -215,19 +217,27 @@ static __device__ __forceinline__ void step_fwd(float &acc, uint32_t &cur, int &
   }
 }
 
-// One step of a ray, backward (prjb.cu:70-77 / :153-178): the same segments, spread as
-// int32 fixed point (acc holds the ray's value times the per-LOR scale).
-static __device__ __forceinline__ void step_bwd(const float acc, uint32_t &cur, int &dz4,
-                                                float &tzc, const int dir4, const float dtz,
-                                                float tn, float tp, float lt, uint32_t off) {
+// Backward: the same segments spread as int32 fixed point (acc holds the ray's value times
+// the per-LOR scale), in two phases so that the rays of a thread run as straight-line
+// code: phase 1 (every ray) adds the part in the current voxel -- weight lt, or
+// (tzc - tp) on a crossing -- and phase 2 (crossing rays only) moves the cursor and adds
+// (tn - tzc) to the new voxel.  (Measured on the forward walk the split was slower, so the
+// forward keeps the one-call step.)
+static __device__ __forceinline__ void step_bwd1(const float acc, const uint32_t cur,
+                                                 const float tzc, float tn, float tp, float lt,
+                                                 uint32_t off) {
+  const float w = (tn > tzc) ? __fsub_rn(tzc, tp) : lt;
+  reds_add_s32(cur + off, __float2int_rn(w * acc));
+}
+
+static __device__ __forceinline__ void step_bwd2(const float acc, uint32_t &cur, int &dz4,
+                                                 float &tzc, const int dir4, const float dtz,
+                                                 float tn, uint32_t off) {
   if (tn > tzc) {
-    reds_add_s32(cur + off, __float2int_rn(__fsub_rn(tzc, tp) * acc));
     cur += dz4;
     dz4 = dir4 - dz4;
     reds_add_s32(cur + off, __float2int_rn(__fsub_rn(tn, tzc) * acc));
     tzc = __fadd_rn(tzc, dtz);
-  } else {
-    reds_add_s32(cur + off, __float2int_rn(lt * acc));
   }
 }
 
@@ -251,11 +261,15 @@ __device__ __forceinline__ void walk_chunk(RayState &S, const void *chunk, const
     for (int u = 0; u < 8; u++) {
       const float tn = t8[u];
       const float lt = __fsub_rn(tn, tp);
+      if (BWD) {
 #pragma unroll
-      for (int r = 0; r < RPT; r++) {
-        if (BWD)
-          step_bwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, tp, lt, u * 512u);
-        else
+        for (int r = 0; r < RPT; r++) step_bwd1(S.acc[r], cur[r], S.tzc[r], tn, tp, lt, u * 512u);
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+          step_bwd2(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, u * 512u);
+      } else {
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
           step_fwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, lt, u * 512u);
       }
       tp = tn;
@@ -266,14 +280,19 @@ __device__ __forceinline__ void walk_chunk(RayState &S, const void *chunk, const
   for (; i < n; i++) {
     const float tn = tnb[i];
     const float lt = __fsub_rn(tn, tp);
+    if (BWD) {
 #pragma unroll
-    for (int r = 0; r < RPT; r++) {
-      if (BWD)
-        step_bwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, tp, lt, 0u);
-      else
+      for (int r = 0; r < RPT; r++) step_bwd1(S.acc[r], cur[r], S.tzc[r], tn, tp, lt, 0u);
+#pragma unroll
+      for (int r = 0; r < RPT; r++)
+        step_bwd2(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, 0u);
+    } else {
+#pragma unroll
+      for (int r = 0; r < RPT; r++)
         step_fwd(S.acc[r], cur[r], S.dz4[r], S.tzc[r], S.dir4[r], S.dtz[r], tn, lt, 0u);
-      cur[r] += 512;
     }
+#pragma unroll
+    for (int r = 0; r < RPT; r++) cur[r] += 512;
     tp = tn;
   }
   S.tp = tp;
