@@ -59,7 +59,7 @@ template <int BS, int CH> struct BSmem {
     return align128(rat_off + (size_t)NOUT * BS * sizeof(float));
   }
   template <int NOUT> __host__ __device__ static constexpr size_t total() {
-    return misc_off<NOUT>() + 64;
+    return misc_off<NOUT>() + 128;
   }
 };
 
@@ -278,7 +278,9 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
   unsigned char *misc = smem_raw + L::template misc_off<NOUT>();
   uint64_t *bars = reinterpret_cast<uint64_t *>(misc);
   int *sflag = reinterpret_cast<int *>(misc + 16);
-  unsigned *smax = reinterpret_cast<unsigned *>(misc + 24);  // [2][BS] -> use [2] per lane set
+  // per-image maxima of the back-projected ray values, double-buffered by LOR parity
+  unsigned *smax = reinterpret_cast<unsigned *>(misc + 24);  // [2][BS]
+  float *sinv = reinterpret_cast<float *>(misc + 64);         // [BS] inverse scales
 
   const int tid = threadIdx.x;
   const bool warp0 = tid < 32;
@@ -286,8 +288,7 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     nb_mbar_init(&bars[0], 1);
     nb_mbar_init(&bars[1], 1);
     *sflag = 0;
-    smax[0] = 0u;
-    smax[1] = 0u;
+    for (int k = 0; k < 2 * BS; k++) smax[k] = 0u;
     nb_fence_mbar_init();
   }
   for (int i = tid; i < 2 * CH * COLF; i += NT) ibuf[i] = 0;
@@ -311,7 +312,6 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
   __syncthreads();
 
   BRay<BS, RPT> S;
-  float inv_scale = 0.f;
   uint32_t phase = 0;
   int j = 0, nlor = 0;
   while (J.valid) {
@@ -327,7 +327,12 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     if (chunk == 0) {
       brays_init<BS, NT, RPT>(a, h, S);
       if (!load) {
-        float m = 0.f;
+        // one fixed-point scale per image: images of one group can differ in count level
+        // by orders of magnitude, and a shared scale would quantise the quieter ones'
+        // neighbours on the loudest one's grid
+        float m[BS];
+#pragma unroll
+        for (int k = 0; k < BS; k++) m[k] = 0.f;
 #pragma unroll
         for (int r = 0; r < RPT; r++) {
           const int ray = tid + NT * r;
@@ -342,26 +347,34 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
           for (int k = 0; k < BS; k++) {
             const float v = (ray < NB_NRAYS) ? rat[o * BS + k] * s : 0.f;
             S.acc[r][k] = v;
-            m = fmaxf(m, fabsf(v));
+            m[k] = fmaxf(m[k], fabsf(v));
           }
         }
-        for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         const int par = nlor & 1;
-        if ((tid & 31) == 0 && m > 0.f) atomicMax(&smax[par], __float_as_uint(m));
-        __syncthreads();
-        const unsigned mb = smax[par];
-        if (tid == 0) smax[par ^ 1] = 0u;
-        float scale = 0.f;
-        inv_scale = 0.f;
-        if (mb != 0u && (mb >> 23) < 255u) {
-          const int e = (int)(mb >> 23) - 126;
-          scale = ldexpf(1.f, a.fxbits - e);
-          inv_scale = ldexpf(1.f, e - a.fxbits);
+#pragma unroll
+        for (int k = 0; k < BS; k++) {
+          for (int o = 16; o; o >>= 1) m[k] = fmaxf(m[k], __shfl_xor_sync(0xffffffffu, m[k], o));
+          if ((tid & 31) == 0 && m[k] > 0.f) atomicMax(&smax[par * BS + k], __float_as_uint(m[k]));
         }
+        __syncthreads();
+        float scale[BS];
+#pragma unroll
+        for (int k = 0; k < BS; k++) {
+          const unsigned mb = smax[par * BS + k];
+          scale[k] = 0.f;
+          float inv = 0.f;
+          if (mb != 0u && (mb >> 23) < 255u) {
+            const int e = (int)(mb >> 23) - 126;
+            scale[k] = ldexpf(1.f, a.fxbits - e);
+            inv = ldexpf(1.f, e - a.fxbits);
+          }
+          if (tid == k) sinv[k] = inv;  // read by this LOR's conversions, after a barrier
+        }
+        if (tid < BS) smax[(par ^ 1) * BS + tid] = 0u;
 #pragma unroll
         for (int r = 0; r < RPT; r++)
 #pragma unroll
-          for (int k = 0; k < BS; k++) S.acc[r][k] *= scale;
+          for (int k = 0; k < BS; k++) S.acc[r][k] *= scale[k];
         ++nlor;
       }
     }
@@ -376,14 +389,16 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
       __syncthreads();
       // int32 [col][BS][128] -> float staging [col][128][BS] (the image layout the bulk
       // reduce adds into), zeroing the accumulators; slot 127 (padding) is not written back
-      const int nv = n * COLF;
+      const int nv = n * NB_COLW;
       for (int x = tid; x < nv; x += NT) {
-        const int c = x / COLF, rem = x - c * COLF;
-        const int slot = rem / BS, k = rem - slot * BS;
-        const int src = c * COLF + k * NB_COLW + slot;
-        const int q = ib[src];
-        fb[x] = slot == 127 ? 0.f : (float)q * inv_scale;
-        ib[src] = 0;
+        const int c = x >> 7, slot = x & 127;
+#pragma unroll
+        for (int k = 0; k < BS; k++) {
+          const int src = c * COLF + k * NB_COLW + slot;
+          const int q = ib[src];
+          fb[c * COLF + slot * BS + k] = slot == 127 ? 0.f : (float)q * sinv[k];
+          ib[src] = 0;
+        }
       }
       nb_fence_proxy_async_smem();
     }

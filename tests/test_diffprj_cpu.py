@@ -37,3 +37,14 @@ def test_image_shape_checks():
         diffprj._as_batch(torch.zeros((320, 320, 128)), cpu)
     with pytest.raises(ValueError):
         diffprj._as_batch(torch.zeros((320, 320, 127), dtype=torch.float64), cpu)
+
+
+def test_dynamic_frame_counts_span_the_range():
+    from nipet_b200 import dynamic
+    c, t0, dur = dynamic.frame_counts(16, seed=0)
+    assert c.shape == (16,) and np.isclose(c.min(), 2e5) and np.isclose(c.max(), 5e7)
+    assert np.all(np.diff(t0) > 0) and np.allclose(t0[1:], np.cumsum(dur)[:-1])
+    c2, _, _ = dynamic.frame_counts(16, seed=0)
+    assert np.array_equal(c, c2)
+    c3, _, _ = dynamic.frame_counts(16, seed=1)
+    assert not np.array_equal(c, c3)
