@@ -3,9 +3,12 @@
 // The voxel a ray visits is decided in float32 with the operation order of the
 // reference kernels (prj/src/prjf.cu:38-39 direct, :136-160 oblique; prjb.cu has the
 // same lines).  Every operation is written with an explicit round-to-nearest intrinsic
-// so the compiler cannot contract or reorder it; the one multiply-add the reference
-// writes as `pz + az_atn * t` is an explicit fused multiply-add, matching nvcc's
-// default contraction of that expression.
+// so the compiler cannot contract or reorder it.  Where nvcc contracts the reference's
+// expressions the restatement fuses explicitly: `pz + az_atn * t`, and the voxel position
+// .5*SZ_IMZ + SZ_VOXZi*z and plane c*SZ_VOXZ - .5*SZ_IMZ*SZ_VOXZ, whose double sums nvcc
+// narrows to float (exact for these operands) and then fuses with the product.  This
+// decides the start voxel of a ray whose position falls on a plane (checked against the
+// reference's own projections on every LOR).
 #pragma once
 #include "nb_internal.cuh"
 
@@ -17,9 +20,12 @@ struct nb_axial {
   float s;     // oblique length factor sqrt(1 + (dz/atn)^2) (1 for direct rays)
 };
 
-// floorf(.5*SZ_IMZ + SZ_VOXZi*z): float product, double sum, rounded to float, floor
+// .5*SZ_IMZ + SZ_VOXZi*z as one fused multiply-add; c*SZ_VOXZ - .5*SZ_IMZ*SZ_VOXZ likewise
 static __device__ __forceinline__ float nb_zpos(float z) {
-  return __double2float_rn(__dadd_rn(0.5 * NB_IMZ, (double)__fmul_rn(NB_VOXZi, z)));
+  return __fmaf_rn(NB_VOXZi, z, (float)(0.5 * NB_IMZ));
+}
+static __device__ __forceinline__ float nb_zline(float c) {
+  return __fmaf_rn(c, NB_VOXZ, (float)(-0.5 * NB_IMZ * (double)NB_VOXZ));
 }
 static __device__ __forceinline__ int nb_zvox(float z) { return (int)floorf(nb_zpos(z)); }
 
@@ -41,15 +47,12 @@ static __device__ __forceinline__ void nb_axial_setup(const nb_ray &R, float atn
   float pz = __double2float_rn(__dadd_rn((double)R.r0z, 0.5 * (double)NB_RING));
   float z = __fmaf_rn(az_atn, tp, pz);
   int w = nb_zvox(z);
-  const double half_extent = 0.5 * NB_IMZ * (double)NB_VOXZ;
-  float lz1 = __double2float_rn(
-      __dsub_rn((double)__fmul_rn(ceilf(nb_zpos(z)), NB_VOXZ), half_extent));
+  float lz1 = nb_zline(ceilf(nb_zpos(z)));
   float zm = __double2float_rn(__dsub_rn(__dadd_rn((double)R.r1z, 0.5 * (double)NB_RING),
                                          (double)__fmul_rn(az_atn, tp)));
   int w_ = nb_zvox(zm);
   float z2 = __fmaf_rn(az_atn, t2, pz);
-  float lz2 = __double2float_rn(
-      __dsub_rn((double)__fmul_rn(floorf(nb_zpos(z2)), NB_VOXZ), half_extent));
+  float lz2 = nb_zline(floorf(nb_zpos(z2)));
   int nz = (int)__fdiv_rn(fabsf(__fsub_rn(lz2, lz1)), NB_VOXZ);
   float tz1 = __fdiv_rn(__fsub_rn(lz1, pz), az_atn);
   float tz2 = __fdiv_rn(__fsub_rn(lz2, pz), az_atn);

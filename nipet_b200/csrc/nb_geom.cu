@@ -50,8 +50,11 @@ __global__ void k_siddon_tx(const float4 *__restrict__ crs, const short2 *__rest
   int v = (int)__dsub_rn(0.5 * NB_IMY, (double)cy1);
   float y2 = __fmaf_rn(aty, t2, py);
   float lr2 = __fmul_rn(NB_VOXY, __fadd_rn(floorf(__fdiv_rn(y2, NB_VOXY)), sgy));
-  float tr1 = __fdiv_rn(__fsub_rn(lr1, py), aty);
-  float tr2 = __fdiv_rn(__fsub_rn(lr2, py), aty);
+  // the compiled reference fuses the boundary line into the offset (lr - py becomes
+  // fma(SZ_VOXY, c, -py)); lr1/lr2 keep the rounded product in their other uses
+  float tr1 = __fdiv_rn(__fmaf_rn(NB_VOXY, __fsub_rn(cy1, sgy), -py), aty);
+  float cy2 = __fadd_rn(floorf(__fdiv_rn(y2, NB_VOXY)), sgy);
+  float tr2 = __fdiv_rn(__fmaf_rn(NB_VOXY, cy2, -py), aty);
   bool y21 = fabsf(__fsub_rn(y2, y1)) >= NB_VOXY;
   bool lr21 = fabsf(__fsub_rn(lr1, lr2)) < NB_L21;
   int nr = (int)__fadd_rn(__fmul_rn((float)y21, roundf(__fdiv_rn(fabsf(__fsub_rn(lr2, lr1)),
@@ -71,7 +74,8 @@ __global__ void k_siddon_tx(const float4 *__restrict__ crs, const short2 *__rest
   float x2 = __fmaf_rn(atx, t2, px);
   float lc2 = __fmul_rn(NB_VOXY, __fadd_rn(floorf(__fdiv_rn(x2, NB_VOXY)), (float)sgx));
   float tc1 = __fdiv_rn(__fsub_rn(lc1, px), atx);
-  float tc2 = __fdiv_rn(__fsub_rn(lc2, px), atx);
+  float tc2 = __fdiv_rn(
+      __fmaf_rn(NB_VOXY, __fadd_rn(floorf(__fdiv_rn(x2, NB_VOXY)), (float)sgx), -px), atx);
   bool x21 = fabsf(__double2float_rn(__dsub_rn((double)x2, x1))) >= NB_VOXY;
   bool lc21 = fabsf(__fsub_rn(lc1, lc2)) < NB_L21;
   int nc = (int)__fadd_rn(__fmul_rn((float)x21, roundf(__fdiv_rn(fabsf(__fsub_rn(lc2, lc1)),

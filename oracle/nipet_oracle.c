@@ -120,12 +120,18 @@ static void siddon_one(const float *crs, const short *s2c, int idx, float *tt, u
   /* rows */
   float y1 = mad(aty, t1, py);
   int sgy = signbit(aty) ? 1 : 0;
-  float lr1 = SZ_VOXY * (ceilf(y1 / SZ_VOXY) - (float)sgy);
+  float cr1 = ceilf(y1 / SZ_VOXY) - (float)sgy;
+  float lr1 = SZ_VOXY * cr1;
   int v = (int)(0.5 * SZ_IMY - (double)ceilf(y1 / SZ_VOXY));
   float y2 = mad(aty, t2, py);
-  float lr2 = SZ_VOXY * (floorf(y2 / SZ_VOXY) + (float)sgy);
-  float tr1 = (lr1 - py) / aty;
-  float tr2 = (lr2 - py) / aty;
+  float cr2 = floorf(y2 / SZ_VOXY) + (float)sgy;
+  float lr2 = SZ_VOXY * cr2;
+  /* the compiled reference fuses the boundary line into the offset: lr - py is
+   * fma(SZ_VOXY, c, -py), the product left unrounded (checked bit for bit against the
+   * reference's own tables on all 68516 LORs); lr1/lr2 keep the rounded product in
+   * their other uses */
+  float tr1 = fmaf(SZ_VOXY, cr1, -py) / aty;
+  float tr2 = fmaf(SZ_VOXY, cr2, -py) / aty;
   int y21 = fabsf(y2 - y1) >= SZ_VOXY;
   int lr21 = fabsf(lr1 - lr2) < L21;
   int nr = (int)((float)y21 * roundf(fabsf(lr2 - lr1) / SZ_VOXY) + (float)lr21);
@@ -140,9 +146,10 @@ static void siddon_one(const float *crs, const short *s2c, int idx, float *tt, u
   float lc1 = (float)((double)SZ_VOXY * (ceil(x1 / (double)SZ_VOXY) - sgx));
   int u = (int)(0.5 * SZ_IMX + floor(x1 / (double)SZ_VOXY));
   float x2 = mad(atx, t2, px);
-  float lc2 = SZ_VOXY * (floorf(x2 / SZ_VOXY) + (float)sgx);
+  float cc2 = floorf(x2 / SZ_VOXY) + (float)sgx;
+  float lc2 = SZ_VOXY * cc2;
   float tc1 = (lc1 - px) / atx;
-  float tc2 = (lc2 - px) / atx;
+  float tc2 = fmaf(SZ_VOXY, cc2, -px) / atx; /* as tr1/tr2 (lc1 is a double: no fusion) */
   int x21 = fabsf((float)((double)x2 - x1)) >= SZ_VOXY;
   int lc21 = fabsf(lc1 - lc2) < L21;
   int nc = (int)((float)x21 * roundf(fabsf(lc2 - lc1) / SZ_VOXY) + (float)lc21);
@@ -260,10 +267,14 @@ typedef struct {
   float tzc, dtz; /* next axial crossing and its increment (float, as the reference) */
 } axial_t;
 
-static inline int zvox(float z) {
-  /* floorf(.5*SZ_IMZ + SZ_VOXZi*z): double sum rounded to float, then floorf */
-  return (int)floorf((float)(.5 * SZ_IMZ + (double)(SZ_VOXZi * z)));
-}
+/* z position in voxels, .5*SZ_IMZ + SZ_VOXZi*z, and a z plane, c*SZ_VOXZ - .5*SZ_IMZ*SZ_VOXZ,
+ * as the compiled reference evaluates them (prjf.cu:150-158, prjb.cu alike): the double
+ * sums are narrowed to float (exact for these operands) and the multiply-add fused, so the
+ * product is not rounded.  This decides which voxel a ray whose position falls on a plane
+ * starts in; checked against the reference's own projections on every LOR. */
+static inline float zpos(float z) { return fmaf(SZ_VOXZi, z, (float)(.5 * SZ_IMZ)); }
+static inline float zline(float c) { return fmaf(c, SZ_VOXZ, (float)(-.5 * SZ_IMZ * SZ_VOXZ)); }
+static inline int zvox(float z) { return (int)floorf(zpos(z)); }
 
 static void axial_setup(const float *li2rng, int ixz, float atn, float tp, float t2,
                         axial_t *A) {
@@ -275,13 +286,11 @@ static void axial_setup(const float *li2rng, int ixz, float atn, float tp, float
   float pz = (float)((double)r0 + .5 * SZ_RING);
   float z = mad(az_atn, tp, pz);
   A->w = zvox(z);
-  float lz1 = (float)((double)(ceilf((float)(.5 * SZ_IMZ + (double)(SZ_VOXZi * z))) * SZ_VOXZ) -
-                      .5 * SZ_IMZ * SZ_VOXZ);
+  float lz1 = zline(ceilf(zpos(z)));
   z = (float)((double)r1 + .5 * SZ_RING - (double)(az_atn * tp));
   A->w_ = zvox(z);
   z = mad(az_atn, t2, pz);
-  float lz2 = (float)((double)(floorf((float)(.5 * SZ_IMZ + (double)(SZ_VOXZi * z))) * SZ_VOXZ) -
-                      .5 * SZ_IMZ * SZ_VOXZ);
+  float lz2 = zline(floorf(zpos(z)));
   int nz = (int)(fabsf(lz2 - lz1) / SZ_VOXZ);
   float tz1 = (lz1 - pz) / az_atn;
   float tz2 = (lz2 - pz) / az_atn;

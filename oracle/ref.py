@@ -1,0 +1,120 @@
+"""Test infrastructure: ctypes binding of the reference's own CUDA projectors and OSEM,
+compiled from the reference sources by `oracle/build_ref.sh` into `oracle/_ref/` (with
+the harness `oracle/ref_harness.cu`).  Used only by tests/ (to pin the oracle and the
+B200 kernels against the reference's output) and by bench.py's reference arm.  Host
+numpy arrays in and out, as the reference's `petprj` calls take them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, '_ref', 'libnipet_ref.so')
+NAW = 68516
+IMG = (320, 320, 127)
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f'{LIB_PATH} is missing (run oracle/build_ref.sh where '
+                                    'the reference sources are present)')
+        lib = C.CDLL(LIB_PATH)
+        P, I = C.c_void_p, C.c_int
+        lib.ref_fprj.argtypes = [P, P, P, I, I, I, P, P, P, P, P, P, I, P]
+        lib.ref_bprj.argtypes = [P, P, P, I, I, P, P, P, P, P, I, P]
+        lib.ref_osem.argtypes = [P, P, P, P, P, P, P, P, I, I, P, P, P, P, P, P, I, I, P]
+        lib.ref_tables.argtypes = [P, P, P, P, I]
+        for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables):
+            f.restype = I
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class _Luts:
+    def __init__(self, params, span):
+        tx, ax = params['txLUT'], params['axLUT']
+        self.li2rng = np.ascontiguousarray(ax['li2rng'], np.float32)
+        self.li2sn = np.ascontiguousarray(ax['li2sn'] if span == 11 else ax['li2sn1'], np.int16)
+        self.li2nos = np.ascontiguousarray(ax['li2nos'], np.int8)
+        self.s2c = np.ascontiguousarray(tx['s2c'], np.int16)
+        self.aw2ali = np.ascontiguousarray(tx['aw2ali'], np.int32)
+        self.crs = np.ascontiguousarray(tx['crs'], np.float32)
+        self.ncrs = int(self.crs.shape[0])
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f'reference {what} failed with CUDA error {rc}')
+
+
+def fprj(params, im, subs=None, span=11, att=0):
+    """Reference gpu_fprj: returns (sino [nprj][nsinos] float32, device ms)."""
+    L = _Luts(params, span)
+    im = np.ascontiguousarray(im, np.float32).reshape(IMG)
+    s = None if subs is None else np.ascontiguousarray(subs, np.int32).reshape(-1)
+    nprj = NAW if s is None else s.size
+    out = np.empty((nprj, 837 if span == 11 else 4084), np.float32)
+    ms = C.c_float()
+    _check(load().ref_fprj(_p(out), _p(im), _p(s), nprj, span, att, _p(L.li2rng), _p(L.li2sn),
+                           _p(L.li2nos), _p(L.s2c), _p(L.aw2ali), _p(L.crs), L.ncrs,
+                           C.byref(ms)), 'fprj')
+    return out, ms.value
+
+
+def bprj(params, sino, subs=None, span=11):
+    """Reference gpu_bprj: returns (image [320][320][127] float32, device ms)."""
+    L = _Luts(params, span)
+    sino = np.ascontiguousarray(sino, np.float32)
+    s = None if subs is None else np.ascontiguousarray(subs, np.int32).reshape(-1)
+    nprj = NAW if s is None else s.size
+    if sino.shape != (nprj, 837 if span == 11 else 4084):
+        raise ValueError('sinogram shape does not match the subset')
+    out = np.empty(IMG, np.float32)
+    ms = C.c_float()
+    _check(load().ref_bprj(_p(out), _p(sino), _p(s), nprj, span, _p(L.li2rng), _p(L.li2sn),
+                           _p(L.li2nos), _p(L.s2c), _p(L.crs), L.ncrs, C.byref(ms)), 'bprj')
+    return out, ms.value
+
+
+def osem(params, img, msk, psng, rsng, ssng, nsng, asng, subs_table, sens, span=11):
+    """One reference OSEM iteration (all subsets), updating `img` in place; returns the
+    time of the call in ms (including the reference's own host<->device copies)."""
+    L = _Luts(params, span)
+    assert img.dtype == np.float32 and img.flags.c_contiguous and img.shape == IMG
+    msk = np.ascontiguousarray(msk, np.uint8)
+    psng = np.ascontiguousarray(psng, np.uint16)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    tab = np.ascontiguousarray(subs_table, np.int32)
+    sens = f32(sens)
+    if sens.shape != (tab.shape[0],) + IMG:
+        raise ValueError('one sensitivity image per subset is required')
+    ms = C.c_float()
+    _check(load().ref_osem(_p(img), _p(msk), _p(psng), _p(f32(rsng)), _p(f32(ssng)),
+                           _p(f32(nsng)), _p(f32(asng)), _p(tab), tab.shape[0], tab.shape[1],
+                           _p(sens), _p(L.li2rng), _p(L.li2sn), _p(L.li2nos), _p(L.s2c),
+                           _p(L.crs), L.ncrs, span, C.byref(ms)), 'osem')
+    return ms.value
+
+
+def tables(params):
+    """Reference gpu_siddon_tx tables: (tt [68516, 10] float32, tv [68516, 1807] uint8)."""
+    L = _Luts(params, 11)
+    tt = np.empty((NAW, 10), np.float32)
+    tv = np.empty((NAW, 1807), np.uint8)
+    _check(load().ref_tables(_p(tt), _p(tv), _p(L.s2c), _p(L.crs), L.ncrs), 'tables')
+    return tt, tv

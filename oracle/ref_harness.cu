@@ -1,0 +1,199 @@
+// Test-only harness around the reference's own CUDA projectors and OSEM.
+//
+// Built by oracle/build_ref.sh together with the reference sources
+// (niftypet/nipet/prj/src/{prjf,prjb,tprj,recon}.cu and niftypet/nipet/src/scanner_0.cu,
+// compiled in place from the reference tree, nothing copied) into oracle/_ref/, and used
+// only by tests/ and bench.py's reference arm to check the oracle and time the reference.
+// The reference's Python glue (prj/src/prj_module.cu) needs the un-vendored `cuvec`
+// package, so these wrappers stand in for its argument handling: host arrays in,
+// device buffers allocated and filled the way prj_module.cu:232-425 (fprj),
+// :430-608 (bprj) and :613-839 (osem) do, the reference routine called, results copied
+// back.  Kernel time is measured with CUDA events around the reference call.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "prjb.h"
+#include "prjf.h"
+#include "recon.h"
+
+namespace {
+
+Cnst make_cnst(int span) {
+  Cnst c;
+  std::memset(&c, 0, sizeof(c));
+  c.SPN = (char)span;
+  c.RNG_STRT = 0;
+  c.RNG_END = NRINGS;
+  c.NRNG = NRINGS;
+  c.NSN1 = NSINOS;
+  c.NSN11 = NSINOS11;
+  c.LOG = LOGWARNING;
+  c.DEVID = 0;
+  return c;
+}
+
+int nsinos(int span) { return span == 11 ? NSINOS11 : NSINOS; }
+
+struct Tx {
+  float4 *crs = nullptr;
+  short2 *s2c = nullptr;
+  float *tt = nullptr;
+  unsigned char *tv = nullptr;
+  int *subs = nullptr;
+  cudaError_t err = cudaSuccess;
+
+  Tx(const float *crs_h, int ncrs, const int16_t *s2c_h, const int *subs_h, int nprj) {
+    chk(cudaMalloc(&crs, ncrs * sizeof(float4)));
+    chk(cudaMemcpy(crs, crs_h, ncrs * sizeof(float4), cudaMemcpyHostToDevice));
+    chk(cudaMalloc(&s2c, AW * sizeof(short2)));
+    chk(cudaMemcpy(s2c, s2c_h, AW * sizeof(short2), cudaMemcpyHostToDevice));
+    chk(cudaMalloc(&tt, (size_t)N_TT * AW * sizeof(float)));
+    chk(cudaMalloc(&tv, (size_t)N_TV * AW));
+    chk(cudaMemset(tv, 0, (size_t)N_TV * AW));
+    chk(cudaMalloc(&subs, (size_t)nprj * sizeof(int)));
+    if (subs_h) {
+      chk(cudaMemcpy(subs, subs_h, (size_t)nprj * sizeof(int), cudaMemcpyHostToDevice));
+    } else {
+      int *all = new int[nprj];
+      for (int i = 0; i < nprj; i++) all[i] = i;
+      chk(cudaMemcpy(subs, all, (size_t)nprj * sizeof(int), cudaMemcpyHostToDevice));
+      delete[] all;
+    }
+  }
+  ~Tx() {
+    cudaFree(crs);
+    cudaFree(s2c);
+    cudaFree(tt);
+    cudaFree(tv);
+    cudaFree(subs);
+  }
+  void chk(cudaError_t e) {
+    if (err == cudaSuccess && e != cudaSuccess) err = e;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Forward projection of `im` ([320][320][127] float, host) into `sino` ([nprj][nsinos]
+// float, host) by the reference's gpu_fprj; subs (host [nprj]) or NULL with nprj = 68516.
+// *ms: device time of the gpu_fprj call (tables + projection kernels).  Returns a
+// cudaError_t code (0 = success).
+int ref_fprj(float *sino, const float *im, const int *subs, int nprj, int span, int att,
+             const float *li2rng, const int16_t *li2sn, const int8_t *li2nos,
+             const int16_t *s2c, const int *aw2ali, const float *crs, int ncrs, float *ms) {
+  const int nsn = nsinos(span);
+  Tx tx(crs, ncrs, s2c, subs, nprj);
+  float *d_im = nullptr, *d_sn = nullptr;
+  tx.chk(cudaMalloc(&d_im, (size_t)SZ_IMX * SZ_IMY * SZ_IMZ * sizeof(float)));
+  tx.chk(cudaMemcpy(d_im, im, (size_t)SZ_IMX * SZ_IMY * SZ_IMZ * sizeof(float),
+                    cudaMemcpyHostToDevice));
+  tx.chk(cudaMalloc(&d_sn, (size_t)nprj * nsn * sizeof(float)));
+  if (tx.err != cudaSuccess) return (int)tx.err;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  gpu_fprj(d_sn, d_im, const_cast<float *>(li2rng), const_cast<short *>(li2sn),
+           reinterpret_cast<char *>(const_cast<int8_t *>(li2nos)), tx.s2c,
+           const_cast<int *>(aw2ali), tx.crs, tx.subs, tx.tt, tx.tv, nprj, AW, make_cnst(span),
+           (char)att, false);
+  cudaEventRecord(e1, 0);
+  tx.chk(cudaEventSynchronize(e1));
+  tx.chk(cudaGetLastError());
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  tx.chk(cudaMemcpy(sino, d_sn, (size_t)nprj * nsn * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_im);
+  cudaFree(d_sn);
+  return (int)tx.err;
+}
+
+// Back projection of `sino` ([nprj][nsinos], host) into `im` ([320][320][127], host,
+// overwritten) by the reference's gpu_bprj.  Arguments as ref_fprj.
+int ref_bprj(float *im, const float *sino, const int *subs, int nprj, int span,
+             const float *li2rng, const int16_t *li2sn, const int8_t *li2nos,
+             const int16_t *s2c, const float *crs, int ncrs, float *ms) {
+  const int nsn = nsinos(span);
+  Tx tx(crs, ncrs, s2c, subs, nprj);
+  float *d_im = nullptr, *d_sn = nullptr;
+  tx.chk(cudaMalloc(&d_im, (size_t)SZ_IMX * SZ_IMY * SZ_IMZ * sizeof(float)));
+  tx.chk(cudaMalloc(&d_sn, (size_t)nprj * nsn * sizeof(float)));
+  tx.chk(cudaMemcpy(d_sn, sino, (size_t)nprj * nsn * sizeof(float), cudaMemcpyHostToDevice));
+  if (tx.err != cudaSuccess) return (int)tx.err;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  gpu_bprj(d_im, d_sn, const_cast<float *>(li2rng), const_cast<short *>(li2sn),
+           reinterpret_cast<char *>(const_cast<int8_t *>(li2nos)), tx.s2c, tx.crs, tx.subs,
+           tx.tt, tx.tv, nprj, make_cnst(span), false);
+  cudaEventRecord(e1, 0);
+  tx.chk(cudaEventSynchronize(e1));
+  tx.chk(cudaGetLastError());
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  tx.chk(cudaMemcpy(im, d_im, (size_t)SZ_IMX * SZ_IMY * SZ_IMZ * sizeof(float),
+                    cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_im);
+  cudaFree(d_sn);
+  return (int)tx.err;
+}
+
+// One OSEM iteration over all subsets by the reference's osem(), updating `img`
+// ([320][320][127], host) in place, as petprj.osem does with PSF off.  subs is the
+// [nsub][nprj1] table (column 0 = projections in the subset, then the LOR indices), sens
+// the [nsub][320][320][127] sensitivity images, msk a [320][320][127] byte mask (0/1),
+// psng [68516][nsinos] uint16, rsng/ssng/nsng/asng [68516][nsinos] float.  *ms: time of
+// the call including the reference's own host<->device transfers.
+int ref_osem(float *img, const uint8_t *msk, const uint16_t *psng, const float *rsng,
+             const float *ssng, const float *nsng, const float *asng, const int *subs, int nsub,
+             int nprj1, const float *sens, const float *li2rng, const int16_t *li2sn,
+             const int8_t *li2nos, const int16_t *s2c, const float *crs, int ncrs, int span,
+             float *ms) {
+  float krnl[3 * KERNEL_LENGTH];
+  for (int i = 0; i < 3 * KERNEL_LENGTH; i++) krnl[i] = -1.f;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  osem(img, reinterpret_cast<bool *>(const_cast<uint8_t *>(msk)),
+       const_cast<unsigned short *>(psng), const_cast<float *>(rsng), const_cast<float *>(ssng),
+       const_cast<float *>(nsng), const_cast<float *>(asng), const_cast<int *>(subs),
+       const_cast<float *>(sens), krnl, const_cast<float *>(li2rng), const_cast<short *>(li2sn),
+       reinterpret_cast<char *>(const_cast<int8_t *>(li2nos)), const_cast<short *>(s2c),
+       const_cast<float *>(crs), nsub, nprj1, ncrs, make_cnst(span));
+  cudaEventRecord(e1, 0);
+  cudaError_t err = cudaEventSynchronize(e1);
+  if (err == cudaSuccess) err = cudaGetLastError();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return (int)err;
+}
+
+// Transaxial Siddon tables of the reference's gpu_siddon_tx (prj/src/tprj.cu): tt
+// [68516][N_TT] float and tv [68516][N_TV] bytes, host.  Returns a cudaError_t code.
+int ref_tables(float *tt, uint8_t *tv, const int16_t *s2c, const float *crs, int ncrs) {
+  Tx tx(crs, ncrs, s2c, nullptr, 1);
+  if (tx.err != cudaSuccess) return (int)tx.err;
+  gpu_siddon_tx(tx.crs, tx.s2c, tx.tt, tx.tv);
+  tx.chk(cudaDeviceSynchronize());
+  tx.chk(cudaGetLastError());
+  tx.chk(cudaMemcpy(tt, tx.tt, (size_t)N_TT * AW * sizeof(float), cudaMemcpyDeviceToHost));
+  tx.chk(cudaMemcpy(tv, tx.tv, (size_t)N_TV * AW, cudaMemcpyDeviceToHost));
+  return (int)tx.err;
+}
+
+}  // extern "C"

@@ -121,3 +121,16 @@ def test_oracle_fprj_span_consistency(oracle, params, span):
     m[ax['li2sn1'][:, 1]] = ax['li2sn'][:, 1]
     np.add.at(acc.T, m, s1.T)
     assert np.allclose(acc, s11, rtol=1e-12, atol=1e-12)
+
+
+def test_oracle_tables_match_reference_tables(params):
+    """The oracle's transaxial Siddon tables against the ones the reference's own CUDA
+    build computed (tests/golden/ref_tables.npz, made by tests/golden/make_ref_tables.py):
+    tt bit for bit, tv by SHA-256."""
+    import hashlib
+    import os
+    from oracle import oracle as O
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'ref_tables.npz'))
+    tt, tv = O.siddon_tables(params['txLUT'])
+    assert np.array_equal(tt.view(np.uint32), g['tt'].view(np.uint32))
+    assert hashlib.sha256(tv.tobytes()).hexdigest() == str(g['tv_sha256'])
