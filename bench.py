@@ -513,33 +513,91 @@ def run_hist(args, ws, rank, dev):
 # reference arm: NIPET has no CPU path; its algorithm restated as the FP64 oracle on the
 # host cores (bounded samples of the same workload)
 # ---------------------------------------------------------------------------------------
+def _reference_cuda_recon(params, scan_host, tab, msk):
+    """One replicate through the reference's own CUDA build (oracle/_ref): 14 gpu_bprj
+    sensitivity images and 4 osem() iterations with host arrays, as mmrrec.osemone drives
+    petprj (prj/mmrrec.py:285-299 and :354).  Returns seconds (wall clock around the
+    calls, which synchronise)."""
+    from oracle import ref
+    h = scan_host
+    an = h['asng'] * h['nsng']
+    t = time.perf_counter()
+    sens = np.stack([ref.bprj(params, an[tab[n, 1:]], tab[n, 1:])[0] for n in range(14)])
+    img = np.ones((320, 320, 127), np.float32)
+    for _ in range(4):
+        ref.osem(params, img, msk, h['psng'], h['rsng'], h['ssng'], h['nsng'], h['asng'], tab,
+                 sens)
+    return time.perf_counter() - t
+
+
 def run_reference(args):
+    """Reference arm.  OSEM workloads: the reference's own CUDA build (compiled from its
+    sources into oracle/_ref) on this GPU, one replicate per step (the reference
+    reconstructs replicates one after another, so its replicate throughput is that of one
+    reconstruction); without that build or a GPU, the FP64 oracle port on the host cores.
+    List-mode workload: the oracle port (bounded sample)."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return None
     from nipet_b200 import geometry
     params = geometry.get_mmrparams()
     metric, unit = METRIC[args.workload]
-    vals = []
+    line = {'impl': 'reference', 'metric': metric, 'unit': unit, 'steps': args.steps,
+            'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'data': 'synthetic'}
+    use_cuda = False
     if args.workload in ('osem', 'batch'):
-        for _ in range(args.warmup + args.steps):
-            vals.append(cpu_osem_sample(params, seconds=6.0))
+        try:
+            import torch
+            from oracle import ref
+            use_cuda = ref.available() and torch.cuda.is_available()
+        except Exception:
+            use_cuda = False
+    if use_cuda:
+        import torch
+        from nipet_b200 import mmrrec
+        dev = torch.device('cuda', 0)
+        scan = mmrrec.synthetic_scan(params, dev, seed=0)
+        host = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
+        del scan
+        torch.cuda.empty_cache()
+        tab = mmrrec.subset_table(params)
+        msk = geometry.get_cylinder(params['Cnt'], rad=29., xo=0, yo=0, unival=1,
+                                    gpu_dim=True) > 0.9
+        ts = [_reference_cuda_recon(params, host, tab, msk)
+              for _ in range(args.warmup + args.steps)][args.warmup:]
+        v = 1.0 / float(np.mean(ts))
+        sample = ('one replicate per step (3e7 counts, span-11, 4 it x 14 subsets + '
+                  '14 sensitivity images) through the reference CUDA build (gpu_bprj, '
+                  'osem) on this GPU, host arrays as petprj takes them')
+        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': 1e3 / v, 'dtype': 'f32',
+                     'config': {'workload': f'{args.workload}: replicates reconstructed one '
+                                            'after another', 'implementation':
+                                'reference CUDA (oracle/_ref), compiled for sm_100a'},
+                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
+                                      'kind': 'reference', 'sample': sample}})
     else:
-        from nipet_b200 import phantoms
-        lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
-        for _ in range(args.warmup + args.steps):
-            vals.append(cpu_hist_sample(lm, params))
-    vals = vals[args.warmup:]
-    v = float(np.mean([x['value'] for x in vals]))
-    cb = dict(vals[-1])
-    cb['value'] = v
-    return {'impl': 'reference', 'metric': metric, 'value': v, 'unit': unit, 'n_gpus': 0,
-            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 / v if unit ==
-            'recon/s' else None, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': {'workload': args.workload, 'implementation': 'FP64 oracle port, OpenMP'},
-            'cpu_baseline': cb, 'e2e': {'value': v, 'unit': unit, 'h2d_bytes_per_step': 0,
-                                        'd2h_bytes_per_step': 0}}
+        vals = []
+        if args.workload in ('osem', 'batch'):
+            for _ in range(args.warmup + args.steps):
+                vals.append(cpu_osem_sample(params, seconds=6.0))
+        else:
+            from nipet_b200 import phantoms
+            lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
+            for _ in range(args.warmup + args.steps):
+                vals.append(cpu_hist_sample(lm, params))
+        vals = vals[args.warmup:]
+        v = float(np.mean([x['value'] for x in vals]))
+        cb = dict(vals[-1])
+        cb['value'] = v
+        line.update({'value': v, 'n_gpus': 0, 'ms_per_step': 1e3 / v if unit == 'recon/s'
+                     else None, 'dtype': 'f64',
+                     'config': {'workload': args.workload,
+                                'implementation': 'FP64 oracle port, OpenMP'},
+                     'cpu_baseline': cb})
+    line['e2e'] = {'value': line['value'], 'unit': unit, 'h2d_bytes_per_step': 0,
+                   'd2h_bytes_per_step': 0}
+    return line
 
 
 def main():

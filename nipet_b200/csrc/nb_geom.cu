@@ -9,6 +9,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
 #include <vector>
 
 #include "nb_axial.cuh"
@@ -310,27 +311,52 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
   }
   // Warp-friendly ray order: the kernels give thread t the rays t, t+NT, ... so every
   // 32-aligned block of ray indices is the lane set of one warp.  Rays of one ring
-  // difference and direction (a "group") sit 2 voxels apart and cross z planes at the same
-  // steps; a warp drawn from one group reads consecutive shared-memory banks and takes
-  // its crossings together.  So each group's full blocks of 32 come first, and the group
-  // remainders (fewer than 32 rays each) are packed after them.
+  // difference d and direction (a "group", 64-|d| rays) sit 2 voxels apart and cross z
+  // planes at the same steps; a warp drawn from one group reads consecutive shared-memory
+  // banks and takes its crossings together.  Order: every group's first 32 rays (groups
+  // of 32 or more), then warps that pair the rest of group d (32-d rays) with all of group
+  // 64-d (d rays) -- exactly 32, at most two groups per warp -- and last the rest of
+  // groups 1..3, which have no partner.  Any ray not placed by these rules (none for the
+  // mMR's 64 rings and maximum ring difference 60) is appended at the end.
   {
     const std::vector<nb_ray> canon = rays;
-    std::vector<int> order, rest;
-    order.reserve(NB_NRAYS);
-    int start = 0;
+    std::map<int, std::vector<int>> grp;  // (kind, d) -> canonical rays in ring order
     auto key = [&](int r) {
       return canon[r].kind * 1000 + (int)lrintf((canon[r].r1z - canon[r].r0z) / NB_RING);
     };
-    for (int r = 1; r <= NB_NRAYS; r++) {
-      if (r == NB_NRAYS || key(r) != key(start)) {
-        const int len = r - start, full = len / 32 * 32;
-        for (int i = 0; i < full; i++) order.push_back(start + i);
-        for (int i = full; i < len; i++) rest.push_back(start + i);
-        start = r;
+    for (int r = 0; r < NB_NRAYS; r++) grp[key(r)].push_back(r);
+    std::vector<int> order;
+    std::vector<char> used(NB_NRAYS, 0);
+    auto take = [&](int k, size_t from, size_t to) {
+      auto it = grp.find(k);
+      if (it == grp.end()) return;
+      for (size_t i = from; i < to && i < it->second.size(); i++) {
+        const int r = it->second[i];
+        if (!used[r]) {
+          used[r] = 1;
+          order.push_back(r);
+        }
       }
-    }
-    order.insert(order.end(), rest.begin(), rest.end());
+    };
+    auto size_of = [&](int k) -> size_t {
+      auto it = grp.find(k);
+      return it == grp.end() ? 0 : it->second.size();
+    };
+    for (auto &kv : grp)  // full first blocks (direct planes: both of theirs)
+      for (size_t f = 0; f + 32 <= kv.second.size(); f += 32)
+        if (kv.first / 1000 == 0 || f == 0) take(kv.first, f, f + 32);
+    for (int kind = 1; kind <= 2; kind++)
+      for (int d = 4; d <= 31; d++) {
+        const int ka = kind * 1000 + d, kb = kind * 1000 + (64 - d);
+        if (size_of(ka) == (size_t)(64 - d) && size_of(kb) == (size_t)d) {
+          take(ka, 32, size_of(ka));
+          take(kb, 0, size_of(kb));
+        }
+      }
+    for (int kind = 1; kind <= 2; kind++)
+      for (int d = 1; d <= 3; d++) take(kind * 1000 + d, 32, size_of(kind * 1000 + d));
+    for (int r = 0; r < NB_NRAYS; r++)
+      if (!used[r]) order.push_back(r);
     for (int r = 0; r < NB_NRAYS; r++) rays[r] = canon[order[r]];
   }
   std::vector<int16_t> bin11(NB_NSN11 * 8, -1), bin1(NB_NSN1, -1);
