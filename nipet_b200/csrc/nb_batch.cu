@@ -59,13 +59,14 @@ template <int BS, int CH> struct BSmem {
     return align128(rat_off + (size_t)NOUT * BS * sizeof(float));
   }
   template <int NOUT> __host__ __device__ static constexpr size_t total() {
-    return misc_off<NOUT>() + 128;
+    return misc_off<NOUT>() + 128;  // barriers, flag, maxima, inverse scales, prefetch cursor
   }
 };
 
 struct BJob {
   int p, g, lor, n, nch, c, valid;
 };
+static_assert(sizeof(BJob) <= 32, "prefetch cursor slot in the misc region");
 
 template <int CH>
 __device__ __forceinline__ void bjob_load(const BatchArgs &a, int q, BJob &J) {
@@ -281,6 +282,10 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
   // per-image maxima of the back-projected ray values, double-buffered by LOR parity
   unsigned *smax = reinterpret_cast<unsigned *>(misc + 24);  // [2][BS]
   float *sinv = reinterpret_cast<float *>(misc + 64);         // [BS] inverse scales
+  // warp 0's prefetch cursor (the job whose chunks it loads ahead) lives in shared memory
+  // so that it takes no registers in the other warps
+  BJob *sP = reinterpret_cast<BJob *>(misc + 80);
+  int *sqP = reinterpret_cast<int *>(misc + 112);
 
   const int tid = threadIdx.x;
   const bool warp0 = tid < 32;
@@ -294,11 +299,12 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
   for (int i = tid; i < 2 * CH * COLF; i += NT) ibuf[i] = 0;
   __syncthreads();
 
-  BJob J, P;
-  int qJ = blockIdx.x, qP = blockIdx.x;
+  BJob J;
+  int qJ = blockIdx.x;
   bjob_load<CH>(a, qJ, J);
   if (warp0) {
-    P = J;
+    BJob P = J;
+    int qP = blockIdx.x;
     for (int k = 0; k < 2 && P.valid; k++) {
       const bool ld = P.c < P.nch;
       const int chunk = ld ? P.c : P.c - P.nch;
@@ -307,6 +313,11 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
       else
         bload_tn<CH>(a, P, chunk, tnbuf + k * CH);
       bjob_next<CH>(a, P, qP);
+    }
+    __syncwarp();
+    if (tid == 0) {
+      *sP = P;
+      *sqP = qP;
     }
   }
   __syncthreads();
@@ -451,6 +462,8 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
           nb_bulk_reduce_add_f32(gb + (size_t)sc[i] * COLF, fb + (size_t)i * COLF, COLF * 4);
       }
       nb_bulk_commit();
+      BJob P = *sP;
+      int qP = *sqP;
       if (P.valid) {
         const bool ld = P.c < P.nch;
         const int pch = ld ? P.c : P.c - P.nch;
@@ -461,6 +474,11 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
           bload_tn<CH>(a, P, pch, tb);
         }
         bjob_next<CH>(a, P, qP);
+      }
+      __syncwarp();
+      if (tid == 0) {
+        *sP = P;
+        *sqP = qP;
       }
     }
     bjob_next<CH>(a, J, qJ);
@@ -603,14 +621,14 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   int st;
   if (span == 11) {
     if (bs == 4)
-      st = launch_batch<4, 16, NB_NSN11, 512, 8>(g, a, s);
+      st = launch_batch<4, 16, NB_NSN11, 1024, 4>(g, a, s);
     else if (bs == 2)
-      st = launch_batch<2, 32, NB_NSN11, 512, 8>(g, a, s);
+      st = launch_batch<2, 32, NB_NSN11, 1024, 4>(g, a, s);
     else
       st = launch_batch<1, 64, NB_NSN11, 1024, 4>(g, a, s);
   } else {
     if (bs == 2)
-      st = launch_batch<2, 32, NB_NSN1, 512, 8>(g, a, s);
+      st = launch_batch<2, 32, NB_NSN1, 1024, 4>(g, a, s);
     else
       st = launch_batch<1, 64, NB_NSN1, 1024, 4>(g, a, s);
   }
