@@ -333,9 +333,9 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     const bool load = J.c < J.nch;
     const int chunk = load ? J.c : J.c - J.nch;
     const int n = max(0, min(CH, J.n - chunk * CH));
-    const float4 h = a.hdr[J.lor];
 
     if (chunk == 0) {
+      const float4 h = a.hdr[J.lor];
       brays_init<BS, NT, RPT>(a, h, S);
       if (!load) {
         // one fixed-point scale per image: images of one group can differ in count level
@@ -415,11 +415,12 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     }
 
     if (load && chunk == J.nch - 1) {
+      const float atn = a.hdr[J.lor].y;
 #pragma unroll
       for (int r = 0; r < RPT; r++) {
         const int ray = tid + NT * r;
         if (ray < NB_NRAYS) {
-          const float s = oblique_s(a.rays[ray], h.y);
+          const float s = oblique_s(a.rays[ray], atn);
 #pragma unroll
           for (int k = 0; k < BS; k++) vals[ray * BS + k] = S.acc[r][k] * s;
         }
