@@ -21,6 +21,7 @@ namespace nbb {
 
 using nbk::WAIT_POLLS;
 using nbk::lds_f32;
+using nbk::nb_fx_round;
 using nbk::reds_add_s32;
 
 constexpr int NB_MAXREP = 1024;
@@ -197,7 +198,7 @@ __device__ __forceinline__ void bstep1(BRay<BS, RPT> &S, int r, uint32_t cur, fl
     // lanes of a warp (neighbouring slots) hit neighbouring banks
 #pragma unroll
     for (int k = 0; k < BS; k++)
-      reds_add_s32(cur + off + 512u * k, __float2int_rn(w * S.acc[r][k]));
+      reds_add_s32(cur + off + 512u * k, nb_fx_round(w, S.acc[r][k]));
   }
 }
 
@@ -217,7 +218,7 @@ __device__ __forceinline__ void bstep2(BRay<BS, RPT> &S, int r, uint32_t &cur, f
     } else {
 #pragma unroll
       for (int k = 0; k < BS; k++)
-        reds_add_s32(cur + off + 512u * k, __float2int_rn(fb * S.acc[r][k]));
+        reds_add_s32(cur + off + 512u * k, nb_fx_round(fb, S.acc[r][k]));
     }
     S.tzc[r] = __fadd_rn(S.tzc[r], S.dtz[r]);
   }

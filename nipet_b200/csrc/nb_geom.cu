@@ -433,9 +433,9 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
     // shared memory by it) and the longest segment sets the fixed-point headroom of the
     // back projector (242 overlapping rays per column slot at most).
     cudaMemset(g->d_err, 0, sizeof(int));
-    nbk::k_check_walk<<<naw, 256>>>(g->d_hdr, g->d_st, g->d_rays, naw, g->d_err);
     unsigned *d_seg = (unsigned *)d_tv;  // reuse the table buffer
     cudaMemset(d_seg, 0, sizeof(unsigned));
+    nbk::k_check_walk<<<naw, 256>>>(g->d_hdr, g->d_st, g->d_rays, naw, g->d_err, d_seg);
     k_maxseg<<<(naw + 255) / 256, 256>>>(g->d_hdr, g->d_st, naw, d_seg);
     unsigned segbits = 0;
     int nbad = 0;
@@ -452,9 +452,16 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
       goto fail;
     }
     memcpy(&g->maxseg, &segbits, sizeof(float));
-    double bound = 242.0 * (g->maxseg > 0.f ? g->maxseg : 1.0);
-    int lb = (int)ceil(log2(bound));
+    // maxseg: the largest weight one ray gives one voxel in one step (the longest step, or
+    // a late crossing's |tzc - tp|).  Slot sums stay below 2^31 (242 rays per slot at
+    // most), and every contribution below 2^22, the range in which the back projectors
+    // round w * value to an integer with one fused multiply-add (nb_fx_round).
+    const double seg = g->maxseg > 0.f ? (double)g->maxseg : 1.0;
+    int lb = (int)ceil(log2(242.0 * seg));
     g->fxbits = 31 - lb;
+    int fm = (int)floor(log2(4194304.0 / seg));
+    while (fm > 0 && ldexp(seg, fm) >= 4194304.0) fm--;
+    if (fm < g->fxbits) g->fxbits = fm;
     if (g->fxbits < 16) {
       nb_set_error_msg("nb_geom_create: walk segments too long (%g cm)", (double)g->maxseg);
       st = NB_ERR_DATA;

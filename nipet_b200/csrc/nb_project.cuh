@@ -192,6 +192,15 @@ static __device__ __forceinline__ float lds_f32(uint32_t addr) {
   asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
   return v;
 }
+// round(x * y) to the nearest integer (ties to even) for |x * y| < 2^22 on the FMA pipe:
+// adding 1.5 * 2^23 inside the fused multiply-add leaves the integer in the low mantissa
+// bits (the classic magic-constant rounding), instead of a multiply and a conversion on the
+// much narrower conversion pipe.  The geometry keeps every back-projection contribution
+// below 2^22 (nb_geom_create's choice of fxbits).
+static __device__ __forceinline__ int nb_fx_round(float x, float y) {
+  return __float_as_int(__fmaf_rn(x, y, 12582912.0f)) - 0x4B400000;
+}
+
 static __device__ __forceinline__ void reds_add_s32(uint32_t addr, int v) {
   asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
@@ -227,7 +236,7 @@ static __device__ __forceinline__ void step_bwd1(const float acc, const uint32_t
                                                  const float tzc, float tn, float tp, float lt,
                                                  uint32_t off) {
   const float w = (tn > tzc) ? __fsub_rn(tzc, tp) : lt;
-  reds_add_s32(cur + off, __float2int_rn(w * acc));
+  reds_add_s32(cur + off, nb_fx_round(w, acc));
 }
 
 static __device__ __forceinline__ void step_bwd2(const float acc, uint32_t &cur, int &dz4,
@@ -236,7 +245,7 @@ static __device__ __forceinline__ void step_bwd2(const float acc, uint32_t &cur,
   if (tn > tzc) {
     cur += dz4;
     dz4 = dir4 - dz4;
-    reds_add_s32(cur + off, __float2int_rn(__fsub_rn(tn, tzc) * acc));
+    reds_add_s32(cur + off, nb_fx_round(__fsub_rn(tn, tzc), acc));
     tzc = __fadd_rn(tzc, dtz);
   }
 }
@@ -497,29 +506,39 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
 // image; it maps to the column's zero padding slot (reads 0, back projections into it
 // are discarded).  In the mMR geometry exactly one ray step reaches it (the last step of
 // rings 59->63 on LOR 24839).  One block per LOR.
+// Walks every ray of every LOR once at geometry creation: counts axial positions outside
+// [0, 127] into *bad, and raises *wbits (float bits, positive) to the largest weight a ray
+// gives its current voxel at a crossing, |tzc - tp| -- which the back projection's
+// fixed-point headroom has to cover besides the longest step.  (A crossing the reference
+// takes a step late, when a ray passes two z planes in one step, makes it negative.)
 static __global__ void k_check_walk(const float4 *__restrict__ hdr, const float *__restrict__ st,
-                             const nb_ray *__restrict__ rays, int naw, int *bad) {
+                                    const nb_ray *__restrict__ rays, int naw, int *bad,
+                                    unsigned *wbits) {
   const int lor = blockIdx.x;
   if (lor >= naw) return;
   const float4 h = hdr[lor];
   const int n = __float_as_int(h.w);
   int nbad = 0;
+  float wmax = 0.f;
   for (int ray = threadIdx.x; ray < NB_NRAYS; ray += blockDim.x) {
     nb_axial A;
     nb_axial_setup(rays[ray], h.y, h.x, h.z, A);
     int w = A.w;
-    float tzc = A.tzc;
+    float tzc = A.tzc, tp = h.x;
     if (w < 0 || w > NB_IMZ) nbad++;
     for (int k = 0; k < n; k++) {
       const float tn = st[(size_t)lor * NB_STEP_STRIDE + k];
       if (tn > tzc) {
+        wmax = fmaxf(wmax, fabsf(__fsub_rn(tzc, tp)));
         w += A.dir;
         tzc = __fadd_rn(tzc, A.dtz);
         if (w < 0 || w > NB_IMZ) nbad++;
       }
+      tp = tn;
     }
   }
   if (nbad) atomicAdd(bad, nbad);
+  if (wmax > 0.f) atomicMax(wbits, __float_as_uint(wmax));
 }
 
 }  // namespace nbk
