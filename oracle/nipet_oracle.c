@@ -268,7 +268,7 @@ typedef struct {
 } axial_t;
 
 /* z position in voxels, .5*SZ_IMZ + SZ_VOXZi*z, and a z plane, c*SZ_VOXZ - .5*SZ_IMZ*SZ_VOXZ,
- * as the compiled reference evaluates them (prjf.cu:150-158, prjb.cu alike): the double
+ * as the compiled reference evaluates them (prjf.cu:39, 148-155, prjb.cu alike): the double
  * sums are narrowed to float (exact for these operands) and the multiply-add fused, so the
  * product is not rounded.  This decides which voxel a ray whose position falls on a plane
  * starts in; checked against the reference's own projections on every LOR. */
