@@ -485,15 +485,24 @@ def run_hist(args, ws, rank, dev):
     clocks = clk.stop() if clk else None
     t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
     nev = int(lm.numel())
-    # e2e: host words -> plan -> device -> histogram -> host sinograms
+    # e2e: pinned host words -> plan -> device -> histogram -> pinned host sinograms
+    lm_pin = torch.from_numpy(lm_host).pin_memory()
+    psn_h = torch.empty((837, 252, 344), dtype=torch.uint16).pin_memory()
+    dsn_h = torch.empty_like(psn_h).pin_memory()
+
+    def e2e_step():
+        p2 = mmr_lmproc.plan(lm_pin.numpy())
+        r = mmr_lmproc.hist_stream(lm_pin, params['txLUT'], params['axLUT'], Cnt, pl=p2)
+        psn_h.copy_(r['psn'])
+        dsn_h.copy_(r['dsn'])
+        torch.cuda.synchronize(dev)
+
+    e2e_step()
     et = []
     for _ in range(max(1, args.e2e_steps)):
+        _barrier(ws, dev)
         t = time.perf_counter()
-        p2 = mmr_lmproc.plan(lm_host)
-        r = mmr_lmproc.hist_stream(lm_host, params['txLUT'], params['axLUT'], Cnt, pl=p2)
-        r['psn'].cpu()
-        r['dsn'].cpu()
-        torch.cuda.synchronize(dev)
+        e2e_step()
         et.append(time.perf_counter() - t)
     te = _max_over_ranks(float(np.mean(et)), ws, dev)
     res = {'ms_per_step': t_step * 1e3, 'value': ws * nev / t_step,
@@ -534,8 +543,9 @@ def run_reference(args):
     """Reference arm.  OSEM workloads: the reference's own CUDA build (compiled from its
     sources into oracle/_ref) on this GPU, one replicate per step (the reference
     reconstructs replicates one after another, so its replicate throughput is that of one
-    reconstruction); without that build or a GPU, the FP64 oracle port on the host cores.
-    List-mode workload: the oracle port (bounded sample)."""
+    reconstruction).  List-mode workload: the reference's lmproc from that build on the
+    same stream written to a file (its input).  Without that build or a GPU, the FP64
+    oracle port on the host cores (bounded samples)."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return None
@@ -546,14 +556,37 @@ def run_reference(args):
             'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'data': 'synthetic'}
     use_cuda = False
-    if args.workload in ('osem', 'batch'):
-        try:
-            import torch
-            from oracle import ref
-            use_cuda = ref.available() and torch.cuda.is_available()
-        except Exception:
-            use_cuda = False
-    if use_cuda:
+    try:
+        import torch
+        from oracle import ref
+        use_cuda = ref.available() and torch.cuda.is_available()
+    except Exception:
+        use_cuda = False
+    if use_cuda and args.workload == 'hist':
+        import torch
+        from nipet_b200 import phantoms
+        from oracle import ref
+        dev = torch.device('cuda', 0)
+        lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=0,
+                                     device=dev).cpu().numpy()
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, 'lm.bf')
+            lm.astype('<i4').tofile(path)
+            ts = []
+            for _ in range(args.warmup + args.steps):
+                t = time.perf_counter()
+                ref.hist(params, path, span=11)
+                ts.append(time.perf_counter() - t)
+        v = lm.size / float(np.mean(ts[args.warmup:]))
+        sample = (f'{lm.size} words over {args.duration} s per step through the reference CUDA '
+                  'build (lmproc: file read, chunking, gpu_hst, span 11) on this GPU')
+        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': lm.size / v * 1e3,
+                     'dtype': 'u32',
+                     'config': {'workload': 'hist', 'implementation':
+                                'reference CUDA (oracle/_ref), compiled for sm_100a'},
+                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
+                                      'kind': 'reference', 'sample': sample}})
+    elif use_cuda and args.workload in ('osem', 'batch'):
         import torch
         from nipet_b200 import mmrrec
         dev = torch.device('cuda', 0)

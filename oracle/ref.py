@@ -1,4 +1,5 @@
-"""Test infrastructure: ctypes binding of the reference's own CUDA projectors and OSEM,
+"""Test infrastructure: ctypes binding of the reference's own CUDA projectors, OSEM and
+list-mode histogrammer,
 compiled from the reference sources by `oracle/build_ref.sh` into `oracle/_ref/` (with
 the harness `oracle/ref_harness.cu`).  Used only by tests/ (to pin the oracle and the
 B200 kernels against the reference's output) and by bench.py's reference arm.  Host
@@ -35,7 +36,10 @@ def load():
         lib.ref_bprj.argtypes = [P, P, P, I, I, P, P, P, P, P, I, P]
         lib.ref_osem.argtypes = [P, P, P, P, P, P, P, P, I, I, P, P, P, P, P, P, I, I, P]
         lib.ref_tables.argtypes = [P, P, P, P, I]
-        for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables):
+        lib.ref_lminfo.argtypes = [C.c_char_p, I, P]
+        lib.ref_hist.argtypes = [C.c_char_p, I, I, I] + [P] * 13 + [P, P, P]
+        for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
+                  lib.ref_hist):
             f.restype = I
         _lib = lib
     return _lib
@@ -118,3 +122,32 @@ def tables(params):
     tv = np.empty((NAW, 1807), np.uint8)
     _check(load().ref_tables(_p(tt), _p(tv), _p(L.s2c), _p(L.crs), L.ncrs), 'tables')
     return tt, tv
+
+
+def hist(params, path, span=11, t0=0, t1=0):
+    """Reference lmproc (no bootstrap) on a list-mode file: returns a dict of host arrays
+    (`psn`, `dsn`, `ssr`, `pvs`, `phc`, `dhc`, `mss`, `fan`, `bck`, `psum`, `dsum`) and the
+    time of the call in ms."""
+    lib = load()
+    nitag = C.c_int()
+    bpath = str(path).encode()
+    _check(lib.ref_lminfo(bpath, 4, C.byref(nitag)), 'lminfo')
+    n = nitag.value
+    nb = {11: 72557856, 1: 354033792, 0: 127 * 86688}[span]
+    tt = (t1 - t0) if t1 > t0 else n
+    sne = (min(n, 5400) + 3) // 4 * 127 * 344
+    out = {'psn': np.zeros(nb, np.uint16), 'dsn': np.zeros(nb, np.uint16),
+           'ssr': np.zeros(127 * 86688, np.uint32), 'pvs': np.zeros(sne, np.uint32),
+           'phc': np.zeros(n, np.uint32), 'dhc': np.zeros(n, np.uint32),
+           'mss': np.zeros(n, np.float32), 'fan': np.zeros(64 * 504, np.uint32),
+           'bck': np.zeros(2 * 224 * n, np.uint32)}
+    tx, ax = params['txLUT'], params['axLUT']
+    s16 = lambda a: np.ascontiguousarray(a, np.int16)  # noqa: E731
+    luts = (s16(tx['s2cF']), s16(ax['sn1_rno']), s16(ax['sn1_sn11']), s16(ax['sn1_ssrb']))
+    psm, dsm, ms = C.c_ulonglong(), C.c_ulonglong(), C.c_float()
+    _check(lib.ref_hist(bpath, t0, t1, span, *[_p(a) for a in luts],
+                        *[_p(out[k]) for k in ('psn', 'dsn', 'ssr', 'pvs', 'phc', 'dhc', 'mss',
+                                               'fan', 'bck')],
+                        C.byref(psm), C.byref(dsm), C.byref(ms)), 'hist')
+    out['psum'], out['dsum'], out['nitag'], out['frame_s'] = psm.value, dsm.value, n, tt
+    return out, ms.value

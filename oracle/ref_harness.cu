@@ -1,19 +1,22 @@
-// Test-only harness around the reference's own CUDA projectors and OSEM.
+// Test-only harness around the reference's own CUDA projectors, OSEM and list-mode
+// histogrammer.
 //
 // Built by oracle/build_ref.sh together with the reference sources
-// (niftypet/nipet/prj/src/{prjf,prjb,tprj,recon}.cu and niftypet/nipet/src/scanner_0.cu,
-// compiled in place from the reference tree, nothing copied) into oracle/_ref/, and used
-// only by tests/ and bench.py's reference arm to check the oracle and time the reference.
-// The reference's Python glue (prj/src/prj_module.cu) needs the un-vendored `cuvec`
-// package, so these wrappers stand in for its argument handling: host arrays in,
-// device buffers allocated and filled the way prj_module.cu:232-425 (fprj),
-// :430-608 (bprj) and :613-839 (osem) do, the reference routine called, results copied
-// back.  Kernel time is measured with CUDA events around the reference call.
+// (niftypet/nipet/prj/src/{prjf,prjb,tprj,recon}.cu, lm/src/{lmproc,hst,lmaux}.cu and
+// src/scanner_0.cu, compiled in place from the reference tree, nothing copied) into
+// oracle/_ref/, and used only by tests/ and bench.py's reference arm to check the oracle
+// and time the reference.  The reference's Python glue (prj/src/prj_module.cu,
+// lm/src/lm_module.cu) needs the un-vendored `cuvec` package, so these wrappers stand in
+// for its argument handling: host arrays in, device buffers allocated and filled the way
+// prj_module.cu:232-425 (fprj), :430-608 (bprj), :613-839 (osem) and
+// lm_module.cu:174-391 (hist) do, the reference routine called, results copied back.
+// Kernel time is measured with CUDA events around the reference call.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <cstring>
 
+#include "lmproc.h"
 #include "prjb.h"
 #include "prjf.h"
 #include "recon.h"
@@ -194,6 +197,83 @@ int ref_tables(float *tt, uint8_t *tv, const int16_t *s2c, const float *crs, int
   tx.chk(cudaMemcpy(tt, tx.tt, (size_t)N_TT * AW * sizeof(float), cudaMemcpyDeviceToHost));
   tx.chk(cudaMemcpy(tv, tx.tv, (size_t)N_TV * AW, cudaMemcpyDeviceToHost));
   return (int)tx.err;
+}
+
+// List-mode file summary by the reference's getLMinfo (lm/src/lmaux.cu): number of
+// one-second time tags.  bpe = bytes per event (4 for the mMR).
+int ref_lminfo(const char *fname, int bpe, int *nitag) {
+  Cnst c = make_cnst(11);
+  c.BPE = bpe;
+  c.LMOFF = 0;
+  getLMinfo(const_cast<char *>(fname), c);
+  *nitag = lmprop.nitag;
+  free(lmprop.atag);
+  free(lmprop.btag);
+  free(lmprop.ele4chnk);
+  free(lmprop.ele4thrd);
+  return (int)cudaGetLastError();
+}
+
+// Histogram of a list-mode file by the reference's lmproc (lm/src/lmproc.cu) without
+// bootstrap, as mmr_lmproc.hist calls it (lm_module.cu:174-391): outputs sized by the
+// caller for nitag time tags -- psn/dsn [tot_bins] uint16, ssr [127*86688], snv [sne],
+// hcp/hcd/mss [nitag], fan [64*504], bck [2*224*nitag].  s2cF [86688][2], sn1_rno
+// [4084][2], sn1_sn11 [4084], sn1_ssrb [4084] (txLUT / axLUT arrays).  *ms: time of
+// the call (file reading included).
+int ref_hist(const char *fname, int tstart, int tstop, int span, const int16_t *s2cF,
+             const int16_t *sn1_rno, const int16_t *sn1_sn11, const int16_t *sn1_ssrb,
+             uint16_t *psn, uint16_t *dsn, uint32_t *ssr, uint32_t *snv, uint32_t *hcp,
+             uint32_t *hcd, float *mss, uint32_t *fan, uint32_t *bck,
+             unsigned long long *psm, unsigned long long *dsm, float *ms) {
+  Cnst c = make_cnst(span);
+  c.BPE = 4;
+  c.LMOFF = 0;
+  c.BTP = 0;
+  c.BTPRT = 1.f;
+  c.W = NSBINS;
+  c.A = NSANGLES;
+  c.NSN1 = NSINOS;
+  axialLUT ax;
+  std::memset(&ax, 0, sizeof(ax));
+  ax.sn1_rno = const_cast<short *>(sn1_rno);
+  ax.sn1_sn11 = const_cast<short *>(sn1_sn11);
+  ax.sn1_ssrb = const_cast<short *>(sn1_ssrb);
+  hstout out;
+  std::memset(&out, 0, sizeof(out));
+  out.psn = psn;
+  out.dsn = dsn;
+  out.ssr = ssr;
+  out.snv = snv;
+  out.hcp = hcp;
+  out.hcd = hcd;
+  out.mss = mss;
+  out.fan = fan;
+  out.bck = bck;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  lmproc(out, const_cast<char *>(fname), tstart, tstop,
+         reinterpret_cast<LORcc *>(const_cast<int16_t *>(s2cF)), ax, c);
+  cudaEventRecord(e1, 0);
+  cudaError_t err = cudaEventSynchronize(e1);
+  if (err == cudaSuccess) err = cudaGetLastError();
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // lmproc fills the counts of its (by-value) output struct only in its own copy: sum here
+  unsigned long long sp = 0, sd = 0;
+  const size_t nb = span == 11 ? (size_t)TOT_BINS : (span == 1 ? (size_t)TOT_BINS_S1
+                                                                 : (size_t)SEG0 * NSBINANG);
+  for (size_t i = 0; i < nb; i++) {
+    sp += psn[i];
+    sd += dsn[i];
+  }
+  if (psm) *psm = sp;
+  if (dsm) *dsm = sd;
+  return (int)err;
 }
 
 }  // extern "C"

@@ -5,7 +5,8 @@ this pins the oracle to what the reference actually computes.
 Bars as in test_gpu_projectors.py: forward projection <= 1e-5 relative per bin (bins at
 least 1e-3 of the maximum; the rest within 1e-8 of the maximum absolutely), back
 projection <= 1e-5 relative L2; one OSEM iteration (14 subsets) of the B200 drop-in
-against the reference's osem(): <= 1e-4 relative L2.
+against the reference's osem(): <= 1e-4 relative L2; Siddon tables and every list-mode
+histogram output (no bootstrap): bit-exact.
 """
 import os
 import sys
@@ -108,3 +109,25 @@ def test_osem_iteration_matches_reference(params, cuda_device):
                 params['Cnt'])
     rl2 = np.linalg.norm(x.astype(np.float64) - x_ref) / np.linalg.norm(x_ref)
     assert rl2 <= 1e-4, f'relative L2 {rl2:.3e}'
+
+
+@pytest.mark.parametrize('nev,dur,span', [(30_000_000, 60, 11), (8_000_000, 20, 1)])
+def test_histogram_bit_exact_with_reference(params, cuda_device, tmp_path, nev, dur, span):
+    """Every output of the list-mode histogram (no bootstrap) against the reference's own
+    lmproc on the same file: prompt/delayed sinograms, SSRB, head curves, centre of mass,
+    projection views, fan sums, bucket singles -- bit for bit.  The span-11 stream spans
+    three of the reference's chunks."""
+    from nipet_b200 import mmr_lmproc, phantoms
+    lm = phantoms.lm_stream_fast(nev, dur, params=params, seed=5, device=cuda_device)
+    lm = lm.cpu().numpy()
+    path = tmp_path / f'lm_span{span}.bf'
+    lm.astype('<i4').tofile(path)
+    r, _ = ref.hist(params, path, span=span)
+    o = mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'],
+                               dict(params['Cnt'], SPN=span, BTP=0))
+    assert int(o['psum']) == r['psum'] and int(o['dsum']) == r['dsum']
+    for k in ('psn', 'dsn', 'ssr', 'phc', 'dhc', 'fan', 'pvs', 'bck'):
+        a = r[k].reshape(-1)
+        b = o[k].cpu().numpy().reshape(-1)[:a.size].astype(a.dtype)
+        assert np.array_equal(a, b), f'{k}: {int(np.sum(a != b))} bins differ'
+    np.testing.assert_array_equal(r['mss'], o['mss'].cpu().numpy().reshape(-1)[:r['mss'].size])
