@@ -42,6 +42,10 @@ if ROOT not in sys.path:
 NAW, NSN11 = 68516, 837
 METRIC = {'batch': ('OSEM recon/s span-11 320\u00b2\u00d7127 (batched+autograd vs plain), '
                     'HBM GB/s vs peak', 'recon/s'),
+          'diff': ('differentiable projector images/s (forward + Poisson NLL + gradient, '
+                   'span-11)', 'images/s'),
+          'dynamic': ('span-1 dynamic frames/s (batched OSEM + per-frame NLL gradient)',
+                      'frames/s'),
           'osem': ('OSEM recon/s span-11 320x320x127 (plain, one scan)', 'recon/s'),
           'hist': ('list-mode histogram events/s', 'events/s')}
 
@@ -457,6 +461,175 @@ def run_batch(args, ws, rank, dev):
 
 
 # ---------------------------------------------------------------------------------------
+# differentiable projector workload
+# ---------------------------------------------------------------------------------------
+def _diff_inputs(params, dev, seed=0, nimg=8):
+    import torch
+    from nipet_b200 import mmrrec, phantoms
+    mu = torch.from_numpy(phantoms.water_mumap()).to(dev)
+    n11 = mmrrec.norm_sinogram_gpu(params, phantoms.crystal_efficiencies(seed), dev)
+    x = torch.stack([torch.from_numpy(phantoms.random_ellipsoids(seed + 10 + b))
+                     for b in range(nimg)]).to(dev) * 20.0
+    return mu, n11, x
+
+
+def run_diff(args, ws, rank, dev):
+    """Batch of 8 images: forward projection with attenuation x normalisation (span 11),
+    Poisson NLL against seeded Poisson data, gradient through the back projector."""
+    import torch
+    from nipet_b200 import diffprj, geometry
+    params = geometry.get_mmrparams()
+    mu, n11, x0 = _diff_inputs(params, dev, seed=rank)
+    prj = diffprj.MMRProjector(params, mu=mu, nsng=n11, span=11, device=dev)
+    g = torch.Generator(device=dev).manual_seed(rank + 1)
+    with torch.no_grad():
+        y = torch.poisson(prj(x0[:1])[0] * 1.2 + 0.1, generator=g)
+    nimg = x0.shape[0]
+
+    def step(x):
+        x = x.detach().requires_grad_(True)
+        loss = diffprj.poisson_nll(prj(x) + 0.1, y.unsqueeze(0), dim=(1, 2)).sum()
+        (gx,) = torch.autograd.grad(loss, x)
+        return loss, gx
+
+    for _ in range(args.warmup):
+        step(x0)
+    prj.check()
+    prj.launches = 0
+    clk = Clocks(dev.index) if rank == 0 else None
+    times = []
+    for _ in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        step(x0)
+        t1.record()
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+    clocks = clk.stop() if clk else None
+    prj.check()
+    launches = prj.launches // max(1, args.steps)
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    # e2e: pinned host images in, host loss and gradients out
+    xh = x0.cpu().pin_memory()
+    gh = torch.empty_like(xh).pin_memory()
+    et = []
+    for k in range(max(1, args.e2e_steps) + 1):
+        _barrier(ws, dev)
+        t = time.perf_counter()
+        loss, gx = step(xh.to(dev, non_blocking=True))
+        gh.copy_(gx)
+        float(loss)
+        torch.cuda.synchronize(dev)
+        if k:
+            et.append(time.perf_counter() - t)
+    te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    # roofline: one step = 2 attenuation projections (weights, recomputed in the backward
+    # pass) + 8 forward + 8 back projections: 4 B per voxel read / update each
+    V = prj.geom.count_reads()
+    achieved = (2 + 2 * nimg) * 4 * V / t_step / 1e9
+    peak, peak_kind = _peaks()
+    res = {'ms_per_step': t_step * 1e3, 'value': ws * nimg / t_step,
+           'e2e': {'value': ws * nimg / te, 'unit': 'images/s',
+                   'h2d_bytes_per_step': int(xh.numel() * 4),
+                   'd2h_bytes_per_step': int(gh.numel() * 4 + 8)},
+           'clocks': clocks, 'gpu_launches': launches,
+           'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                        'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
+                        'kernel': 'k_project forward + back (nb_fprj / nb_bprj), whole step'},
+           'config': {'workload': f'differentiable projector: {nimg} images 320x320x127, '
+                                  'span-11 forward with attenuation x normalisation, Poisson '
+                                  'NLL, gradient by the back projector', 'global_batch':
+                      ws * nimg, 'parallelism': f'replicas x{ws}',
+                      'l2': 'inputs larger than L2'}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb = cpu_osem_sample(params)
+        # the sample's reconstruction is 4.5 x (forward + back projection over all LORs)
+        cb = dict(cb, value=cb['value'] * 4.5, unit='images/s',
+                  sample=cb['sample'] + '; one image = 1 forward + 1 back projection')
+        res['cpu_baseline'] = cb
+    return res
+
+
+# ---------------------------------------------------------------------------------------
+# span-1 dynamic frames workload
+# ---------------------------------------------------------------------------------------
+def run_dynamic(args, ws, rank, dev):
+    """16 span-1 frames (2e5 .. 5e7 counts from a seeded time-activity curve) reconstructed
+    together (4 it x 14 subsets), then each frame's Poisson-NLL gradient via autograd."""
+    import torch
+    from nipet_b200 import dynamic, geometry
+    params = geometry.get_mmrparams()
+    counts, _, _ = dynamic.frame_counts(16, seed=rank)
+    scan = dynamic.dynamic_scan(params, dev, counts, seed=rank)
+    dyn = dynamic.DynamicRecon(params, scan)
+    nfr = dyn.nframes
+
+    def step():
+        dyn.run(niter=4)
+        return dyn.nll_gradients()
+
+    for _ in range(args.warmup):
+        step()
+    dyn.rec.geom.check()
+    dyn.rec.launches = 0
+    dyn.launches = 0
+    clk = Clocks(dev.index) if rank == 0 else None
+    times = []
+    for _ in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        step()
+        t1.record()
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+    clocks = clk.stop() if clk else None
+    dyn.rec.geom.check()
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    # e2e: pinned host prompts in, host frames and gradients out
+    ph = scan['psng'].cpu().pin_memory()
+    img_h = torch.empty((nfr, 320, 320, 127)).pin_memory()
+    grad_h = torch.empty_like(img_h).pin_memory()
+    et = []
+    for k in range(max(1, args.e2e_steps) + 1):
+        _barrier(ws, dev)
+        t = time.perf_counter()
+        s2 = dict(scan, psng=ph.to(dev, non_blocking=True))
+        d2 = dynamic.DynamicRecon(params, s2, bs=dyn.rec.bs).run(niter=4, use_graph=False)
+        x = d2.images()
+        _, g = d2.nll_gradients(x)
+        img_h.copy_(x)
+        grad_h.copy_(g)
+        torch.cuda.synchronize(dev)
+        if k:
+            et.append(time.perf_counter() - t)
+        del d2, s2, x, g
+    te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    res = {'ms_per_step': t_step * 1e3, 'value': ws * nfr / t_step,
+           'e2e': {'value': ws * nfr / te, 'unit': 'frames/s',
+                   'h2d_bytes_per_step': int(ph.numel() * 2),
+                   'd2h_bytes_per_step': int(2 * img_h.numel() * 4)},
+           'clocks': clocks,
+           'gpu_launches': (dyn.rec.launches + dyn.launches) // max(1, args.steps),
+           'roofline': None,
+           'config': {'workload': f'span-1 dynamic: {nfr} frames '
+                                  f'({counts.min():.0e}..{counts.max():.0e} counts), 4084 '
+                                  'sinograms, 320x320x127, 4 it x 14 subsets batched, per-frame '
+                                  'Poisson-NLL gradient by autograd',
+                      'global_batch': ws * nfr, 'batch_width': dyn.rec.bs,
+                      'parallelism': f'replicas x{ws}', 'l2': 'inputs larger than L2'}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb = cpu_osem_sample(params)
+        res['cpu_baseline'] = dict(cb, unit='frames/s',
+                                   sample=cb['sample'] + ' (span-11 sample for a span-1 frame: '
+                                   'the same ray walks)')
+    return res
+
+
+# ---------------------------------------------------------------------------------------
 # list-mode histogram workload
 # ---------------------------------------------------------------------------------------
 def run_hist(args, ws, rank, dev):
@@ -586,6 +759,78 @@ def run_reference(args):
                                 'reference CUDA (oracle/_ref), compiled for sm_100a'},
                      'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
                                       'kind': 'reference', 'sample': sample}})
+    elif use_cuda and args.workload == 'diff':
+        import torch
+        from oracle import ref
+        dev = torch.device('cuda', 0)
+        mu, n11, x0 = _diff_inputs(params, dev)
+        mu_h, n_h, xs = mu.cpu().numpy(), n11.cpu().numpy(), x0.cpu().numpy()
+        del mu, n11, x0
+        y = np.random.default_rng(1).poisson(
+            ref.fprj(params, xs[0])[0] * 1.2 + 0.1).astype(np.float32)
+
+        def one_image(x):
+            a = ref.fprj(params, mu_h, att=1)[0]          # weights, as the forward model
+            w = a * n_h
+            ybar = ref.fprj(params, x)[0] * w + 0.1
+            g = (1.0 - y / ybar) * w
+            return ref.bprj(params, g.astype(np.float32))[0]
+
+        ts = []
+        for k in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            one_image(xs[k % xs.shape[0]])
+            ts.append(time.perf_counter() - t)
+        v = 1.0 / float(np.mean(ts[args.warmup:]))
+        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': 1e3 / v, 'dtype': 'f32',
+                     'config': {'workload': 'diff: one image per step (attenuation '
+                                'projection, forward projection, NLL gradient on the host, '
+                                'back projection)', 'implementation':
+                                'reference CUDA (oracle/_ref), compiled for sm_100a'},
+                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
+                                      'kind': 'reference', 'sample': 'one image per step '
+                                      'through gpu_fprj x2 and gpu_bprj with host arrays'}})
+    elif use_cuda and args.workload == 'dynamic':
+        import torch
+        from nipet_b200 import dynamic, mmrrec
+        from oracle import ref
+        dev = torch.device('cuda', 0)
+        sc = dynamic.dynamic_scan(params, dev, [3e6], seed=0)
+        an, nsng = sc['an'].cpu().numpy(), sc['nsng'].cpu().numpy()
+        psng = sc['psng'][0].cpu().numpy()
+        asng = np.where(np.abs(nsng) > 0, an / np.where(nsng == 0, 1, nsng), 0).astype(np.float32)
+        rsng = np.full_like(an, float(sc['rscale'][0]))
+        ssng = np.zeros_like(an)
+        del sc
+        torch.cuda.empty_cache()
+        tab = mmrrec.subset_table(params)
+        msk = geometry.get_cylinder(params['Cnt'], rad=29., xo=0, yo=0, unival=1,
+                                    gpu_dim=True) > 0.9
+
+        def one_frame():
+            sens = np.stack([ref.bprj(params, an[tab[n, 1:]], tab[n, 1:], span=1)[0]
+                             for n in range(14)])
+            img = np.ones((320, 320, 127), np.float32)
+            for _ in range(4):
+                ref.osem(params, img, msk, psng, rsng, ssng, nsng, asng, tab, sens, span=1)
+            ybar = ref.fprj(params, img, span=1)[0] * an + rsng
+            g = (1.0 - psng / ybar) * an
+            return ref.bprj(params, g.astype(np.float32), span=1)[0]
+
+        ts = []
+        for _ in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            one_frame()
+            ts.append(time.perf_counter() - t)
+        v = 1.0 / float(np.mean(ts[args.warmup:]))
+        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': 1e3 / v, 'dtype': 'f32',
+                     'config': {'workload': 'dynamic: one span-1 frame (3e6 counts) per step, '
+                                '4 it x 14 subsets + sensitivity + one NLL gradient',
+                                'implementation': 'reference CUDA (oracle/_ref), compiled for '
+                                'sm_100a'},
+                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
+                                      'kind': 'reference', 'sample': 'one frame per step '
+                                      'through gpu_bprj, osem, gpu_fprj with host arrays'}})
     elif use_cuda and args.workload in ('osem', 'batch'):
         import torch
         from nipet_b200 import mmrrec
@@ -611,9 +856,11 @@ def run_reference(args):
                                       'kind': 'reference', 'sample': sample}})
     else:
         vals = []
-        if args.workload in ('osem', 'batch'):
+        if args.workload in ('osem', 'batch', 'diff', 'dynamic'):
+            f = 4.5 if args.workload == 'diff' else 1.0  # images per reconstruction's work
             for _ in range(args.warmup + args.steps):
-                vals.append(cpu_osem_sample(params, seconds=6.0))
+                c = cpu_osem_sample(params, seconds=6.0)
+                vals.append(dict(c, value=c['value'] * f, unit=unit))
         else:
             from nipet_b200 import phantoms
             lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
@@ -623,7 +870,7 @@ def run_reference(args):
         v = float(np.mean([x['value'] for x in vals]))
         cb = dict(vals[-1])
         cb['value'] = v
-        line.update({'value': v, 'n_gpus': 0, 'ms_per_step': 1e3 / v if unit == 'recon/s'
+        line.update({'value': v, 'n_gpus': 0, 'ms_per_step': 1e3 / v if unit != 'events/s'
                      else None, 'dtype': 'f64',
                      'config': {'workload': args.workload,
                                 'implementation': 'FP64 oracle port, OpenMP'},
@@ -639,7 +886,8 @@ def main():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='batch', choices=['batch', 'osem', 'hist'])
+    ap.add_argument('--workload', default='batch',
+                    choices=['batch', 'osem', 'hist', 'diff', 'dynamic'])
     ap.add_argument('--replicates', type=int, default=50)
     ap.add_argument('--plain-steps', type=int, default=1)
     ap.add_argument('--e2e-steps', type=int, default=1)
@@ -658,7 +906,8 @@ def main():
     ws, rank, local = _dist()
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    run = {'batch': run_batch, 'osem': run_osem, 'hist': run_hist}[args.workload]
+    run = {'batch': run_batch, 'osem': run_osem, 'hist': run_hist, 'diff': run_diff,
+           'dynamic': run_dynamic}[args.workload]
     res = run(args, ws, rank, dev)
     metric, unit = METRIC[args.workload]
     if rank == 0:

@@ -68,6 +68,7 @@ class MMRProjector:
         self.nsng = None if nsng is None else to_device(nsng, np.float32, dev)
         if self.nsng is not None and tuple(self.nsng.shape) != (NAW, self.nsn):
             raise ValueError(f'nsng must have shape {(NAW, self.nsn)}')
+        self.launches = 0  # kernels launched (layout conversion + projector per image)
 
     # -- the raw projection pair (no weights) ---------------------------------------------
     def _subs_ptr(self):
@@ -80,6 +81,7 @@ class MMRProjector:
         for b in range(x.shape[0]):
             _lib.check(self.lib.nb_fprj(self.geom.handle, dev_ptr(out[b]), dev_ptr(x[b]),
                                         self._subs_ptr(), self.nprj, self.span, att, st))
+            self.launches += 2
         return out
 
     def backproject(self, s: torch.Tensor) -> torch.Tensor:
@@ -89,6 +91,7 @@ class MMRProjector:
         for b in range(s.shape[0]):
             _lib.check(self.lib.nb_bprj(self.geom.handle, dev_ptr(out[b]), dev_ptr(s[b]),
                                         self._subs_ptr(), self.nprj, self.span, st))
+            self.launches += 2
         return out
 
     def weights(self):

@@ -105,6 +105,7 @@ class DynamicRecon:
         self.rec = batch.BatchRecon(params, scan['psng'], scan['rs'], scan['an'],
                                     rscale=scan['rscale'], device=self.device, span=1, bs=bs,
                                     nsub=nsub)
+        self.launches = 0  # projector kernels of the NLL gradients (the OSEM's: rec.launches)
 
     def run(self, niter: int = 4, use_graph: bool = True):
         self.rec.run(niter=niter, use_graph=use_graph)
@@ -135,4 +136,5 @@ class DynamicRecon:
             grad[k0:k1] = g
             del y, loss, g, x
         prj.check()
+        self.launches += prj.launches
         return nll, grad
