@@ -409,7 +409,7 @@ def run_batch(args, ws, rank, dev):
         r2 = batch.BatchRecon(params, host_psng.to(dev, non_blocking=True),
                               host_rs.to(dev, non_blocking=True),
                               host_an.to(dev, non_blocking=True), rscale=rscale, device=dev,
-                              bs=br.bs)
+                              bs=br.bs, tile=br.tile)
         r2.run(niter=4, use_graph=False)
         m, s = r2.mean_std()
         m, s = m.cpu(), s.cpu()
@@ -444,14 +444,15 @@ def run_batch(args, ws, rank, dev):
         'gpu_launches': launches_per_step, 'plain_dropin': plain,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'traffic': traffic,
-                     'kernel': f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk)',
+                     'kernel': f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk, '
+                               f'tile {br.tile})',
                      'peak_kind': peak_kind, 'bytes_per_launch_avg': bytes_iter / len(br.subs),
                      'launch_ms_avg': t_it * 1e3 / len(br.subs)},
         'config': {'workload': f'batched bootstrap OSEM, {nrep} replicates '
                                f'({nrep - nlow} at 3e7, {nlow} at 3e6 counts), span-11 '
                                f'837x252x344, 320x320x127 f32, 4 it x 14 subsets + '
                                f'sensitivity, CUDA graph per iteration',
-                   'global_batch': ws * nrep, 'batch_width': br.bs,
+                   'global_batch': ws * nrep, 'batch_width': br.bs, 'tile': br.tile,
                    'parallelism': f'replicas x{ws}', 'l2': 'inputs larger than L2 '
                    f'({nrep} prompt sinograms, {nrep} images)'},
     }
@@ -598,7 +599,8 @@ def run_dynamic(args, ws, rank, dev):
         _barrier(ws, dev)
         t = time.perf_counter()
         s2 = dict(scan, psng=ph.to(dev, non_blocking=True))
-        d2 = dynamic.DynamicRecon(params, s2, bs=dyn.rec.bs).run(niter=4, use_graph=False)
+        d2 = dynamic.DynamicRecon(params, s2, bs=dyn.rec.bs, tile=dyn.rec.tile).run(
+            niter=4, use_graph=False)
         x = d2.images()
         _, g = d2.nll_gradients(x)
         img_h.copy_(x)
@@ -620,6 +622,7 @@ def run_dynamic(args, ws, rank, dev):
                                   'sinograms, 320x320x127, 4 it x 14 subsets batched, per-frame '
                                   'Poisson-NLL gradient by autograd',
                       'global_batch': ws * nfr, 'batch_width': dyn.rec.bs,
+                      'tile': dyn.rec.tile,
                       'parallelism': f'replicas x{ws}', 'l2': 'inputs larger than L2'}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_osem_sample(params)

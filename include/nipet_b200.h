@@ -134,14 +134,18 @@ int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens1
  *   psng       dev [nrep][68516][nsinos] uint16 prompts; rs dev [68516][nsinos] float
  *              (r+s)/(an) from nb_osem_rs; rscale dev [nrep] per-image randoms factor
  *   bs         1, 2 or 4 (4: span 11 only); span 11 (837 sinograms) or 1 (4084)
+ *   tile       kernel shape: 0 = 1024 threads x 4 rays each, 64/bs columns of the LOR
+ *              staged per shared-memory chunk; 1 = the same threads, 32/bs columns per
+ *              chunk; 2 = 512 threads x 8 rays, 64/bs columns.  Results agree to rounding;
+ *              batch.autotune picks (bs, tile) by timing them.
  * nb_to_batch / nb_from_batch convert nrep reference-layout images [nrep][320][320][127]
  * to and from that layout. */
 int nb_to_batch(float *dst, const float *src, int nrep, int bs, void *stream);
 int nb_from_batch(float *dst, const float *src, int nrep, int bs, void *stream);
 int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens128,
                          const uint8_t *msk128, const uint16_t *psng, const float *rs,
-                         const float *rscale, int nrep, int bs, int span, const int32_t *subs,
-                         int nprj, void *stream);
+                         const float *rscale, int nrep, int bs, int tile, int span,
+                         const int32_t *subs, int nprj, void *stream);
 
 /* ---- list-mode histogramming (lm/src/lmproc.cu:12-230, hst.cu:37-528, lmaux.cu:17-270) -
  * nb_lm_plan replaces getLMinfo + modifyLMinfo: the chunk plan of a list-mode stream

@@ -5,8 +5,9 @@ per-subset sensitivity images; each has its own prompts and a randoms level
 (`rscale[b]` times a common (r+s)/(an) sinogram).  One sub-iteration of all images is one
 persistent kernel launch (`nb_osem_batch_subset`), and a full iteration (14 sub-iterations)
 can be captured once as a CUDA graph and replayed.  The batch width `bs` (images sharing
-one walk of the Siddon geometry) is chosen by `autotune` by timing the candidates on the
-device, and cached per device.
+one walk of the Siddon geometry) and the kernel's tile shape (columns of the LOR staged
+per shared-memory chunk, rays per thread) are chosen by `autotune`, which times the
+candidates on the device and caches the choice per device.
 """
 from __future__ import annotations
 
@@ -44,7 +45,7 @@ class BatchRecon:
 
     def __init__(self, params: dict, psng: torch.Tensor, rs: torch.Tensor, an: torch.Tensor,
                  rscale=None, device=None, span: int = 11, bs: int | None = None,
-                 nsub: int = 14, mask_radius: float = 29.0):
+                 nsub: int = 14, mask_radius: float = 29.0, tile: int | None = None):
         self.device = torch.device(device or psng.device)
         self.params = params
         self.span = int(span)
@@ -71,7 +72,12 @@ class BatchRecon:
         self.sens128 = torch.empty((self.nsub, COL128), device=dev)
         self.graph = None
         self.launches = 0
-        self.bs = int(bs) if bs else autotune(self)
+        if bs:
+            self.bs, self.tile = int(bs), int(tile or 0)
+        else:
+            self.bs, self.tile = autotune(self)
+            if tile is not None:
+                self.tile = int(tile)
         self._alloc()
 
     def _alloc(self):
@@ -100,7 +106,7 @@ class BatchRecon:
         _lib.check(self.lib.nb_osem_batch_subset(
             self.geom.handle, dev_ptr(self.img), dev_ptr(self.bimg), dev_ptr(self.sens128[i]),
             dev_ptr(self.msk128), dev_ptr(self.psng), dev_ptr(self.rs), dev_ptr(self.rscale),
-            self.nrep, self.bs, self.span, dev_ptr(self.subs[i]), self.nprj, st))
+            self.nrep, self.bs, self.tile, self.span, dev_ptr(self.subs[i]), self.nprj, st))
         self.launches += 2
 
     def iteration(self, use_graph: bool = True):
@@ -160,29 +166,36 @@ def _cache_file():
     return os.path.join(d, 'autotune.json')
 
 
-def autotune(rec: BatchRecon, candidates=None, repeats: int = 2) -> int:
-    """Pick the batch width (images per Siddon walk) with the best images/s for this
-    device, span and batch size, timing `repeats` sub-iterations per candidate.  Results
-    are cached in memory and in `~/.cache/nipet_b200/autotune.json`."""
+TILES = (0, 1, 2)
+
+
+def autotune(rec: BatchRecon, candidates=None, repeats: int = 2):
+    """Pick the batch width (images per Siddon walk) and tile shape (see
+    `nb_osem_batch_subset`) with the best images/s for this device, span and batch size,
+    timing `repeats` sub-iterations per candidate after one warm-up.  Returns (bs, tile);
+    results are cached in memory and in `~/.cache/nipet_b200/autotune.json`."""
     name = torch.cuda.get_device_name(rec.device)
     key = f'{name}|span{rec.span}|n{rec.nrep}'
     if key in _TUNE_CACHE:
         return _TUNE_CACHE[key]
+    disk = {}
     try:
         with open(_cache_file()) as f:
             disk = json.load(f)
-        if key in disk:
-            _TUNE_CACHE[key] = int(disk[key])
+        v = disk.get(key)
+        if isinstance(v, list) and len(v) == 2:
+            _TUNE_CACHE[key] = (int(v[0]), int(v[1]))
             return _TUNE_CACHE[key]
     except Exception:
         disk = {}
     if candidates is None:
-        candidates = [1, 2, 4] if rec.span == 11 else [1, 2]
-    candidates = [c for c in candidates if c <= max(1, rec.nrep) or c == 1]
+        widths = [1, 2, 4] if rec.span == 11 else [1, 2]
+        widths = [w for w in widths if w <= max(1, rec.nrep) or w == 1]
+        candidates = [(w, t) for w in widths for t in TILES]
     best, best_t = candidates[0], float('inf')
     rec.sens128.fill_(1.0)
-    for bs in candidates:
-        rec.bs = bs
+    for bs, tile in candidates:
+        rec.bs, rec.tile = bs, tile
         rec._alloc()
         rec.init_images()
         rec.subiteration(0)           # warm-up (also sets kernel attributes)
@@ -196,15 +209,15 @@ def autotune(rec: BatchRecon, candidates=None, repeats: int = 2) -> int:
         torch.cuda.synchronize(rec.device)
         t = e0.elapsed_time(e1)
         if t < best_t:
-            best, best_t = bs, t
+            best, best_t = (bs, tile), t
     rec.geom.check()
     _TUNE_CACHE[key] = best
     try:
         os.makedirs(os.path.dirname(_cache_file()), exist_ok=True)
-        disk[key] = best
+        disk[key] = list(best)
         with open(_cache_file(), 'w') as f:
             json.dump(disk, f, indent=1)
     except Exception:
         pass
-    rec.bs = best
+    rec.bs, rec.tile = best
     return best

@@ -587,8 +587,8 @@ extern "C" int nb_from_batch(float *dst, const float *src, int nrep, int bs, voi
 
 extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens128,
                                     const uint8_t *msk128, const uint16_t *psng, const float *rs,
-                                    const float *rscale, int nrep, int bs, int span,
-                                    const int32_t *subs, int nprj, void *stream) {
+                                    const float *rscale, int nrep, int bs, int tile,
+                                    int span, const int32_t *subs, int nprj, void *stream) {
   NB_REQUIRE(g != nullptr, "nb_osem_batch_subset: NULL geometry handle");
   NB_REQUIRE(img && bimg && sens128 && msk128 && psng && rs && rscale && subs,
              "nb_osem_batch_subset: NULL argument");
@@ -596,6 +596,7 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   NB_REQUIRE(span == 11 || span == 1, "nb_osem_batch_subset: span must be 1 or 11");
   NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
              "nb_osem_batch_subset: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(tile >= 0 && tile <= 2, "nb_osem_batch_subset: tile must be 0, 1 or 2");
   NB_REQUIRE(nprj > 0, "nb_osem_batch_subset: empty subset");
   NB_CUDA(cudaSetDevice(g->device));
   cudaStream_t s = (cudaStream_t)stream;
@@ -620,20 +621,27 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   a.rscale = rscale;
   a.fxbits = g->fxbits;
   a.err = g->d_err;
+  // kernel shape per (span, bs, tile): columns per staged chunk (CH), threads (NT) and
+  // rays per thread (RPT); CH * 128 * bs floats per chunk buffer
+#define NB_TILES(BS, CH, NOUT)                                                            \
+  (tile == 0   ? launch_batch<BS, CH, NOUT, 1024, 4>(g, a, s)                             \
+   : tile == 1 ? launch_batch<BS, CH / 2, NOUT, 1024, 4>(g, a, s)                         \
+               : launch_batch<BS, CH, NOUT, 512, 8>(g, a, s))
   int st;
   if (span == 11) {
     if (bs == 4)
-      st = launch_batch<4, 16, NB_NSN11, 1024, 4>(g, a, s);
+      st = NB_TILES(4, 16, NB_NSN11);
     else if (bs == 2)
-      st = launch_batch<2, 32, NB_NSN11, 1024, 4>(g, a, s);
+      st = NB_TILES(2, 32, NB_NSN11);
     else
-      st = launch_batch<1, 64, NB_NSN11, 1024, 4>(g, a, s);
+      st = NB_TILES(1, 64, NB_NSN11);
   } else {
     if (bs == 2)
-      st = launch_batch<2, 32, NB_NSN1, 1024, 4>(g, a, s);
+      st = NB_TILES(2, 32, NB_NSN1);
     else
-      st = launch_batch<1, 64, NB_NSN1, 1024, 4>(g, a, s);
+      st = NB_TILES(1, 64, NB_NSN1);
   }
+#undef NB_TILES
   if (st) return st;
   k_update_batch<<<g->nsm * 16, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups, bs);
   NB_CUDA(cudaGetLastError());

@@ -93,18 +93,18 @@ class DynamicRecon:
     """Batched span-1 OSEM of all frames of a `dynamic_scan`, then per-frame Poisson
     log-likelihood gradients through `diffprj.MMRProjector`.
 
-    bs (frames per walk of the geometry, 1 or 2 at span 1) is picked by the batch
-    autotuner when None."""
+    bs (frames per walk of the geometry, 1 or 2 at span 1) and the kernel tile are picked
+    by the batch autotuner when None."""
 
     def __init__(self, params: dict, scan: dict, device=None, bs: int | None = None,
-                 nsub: int = 14):
+                 nsub: int = 14, tile: int | None = None):
         self.device = torch.device(device or scan['psng'].device)
         self.params = params
         self.scan = scan
         self.nframes = int(scan['psng'].shape[0])
         self.rec = batch.BatchRecon(params, scan['psng'], scan['rs'], scan['an'],
                                     rscale=scan['rscale'], device=self.device, span=1, bs=bs,
-                                    nsub=nsub)
+                                    nsub=nsub, tile=tile)
         self.launches = 0  # projector kernels of the NLL gradients (the OSEM's: rec.launches)
 
     def run(self, niter: int = 4, use_graph: bool = True):

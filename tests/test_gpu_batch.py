@@ -57,8 +57,26 @@ def test_batch_cuda_graph_replay(params, scan, replicates, cuda_device):
     assert np.isclose(float(m.sum()), float(y.mean(0).sum()), rtol=1e-5)
 
 
-def test_autotune_picks_a_valid_width(params, scan, replicates, cuda_device):
+@pytest.mark.parametrize('bs,tile', [(4, 1), (4, 2), (2, 1), (2, 2), (1, 1), (1, 2)])
+def test_tile_shapes_agree(params, scan, replicates, cuda_device, bs, tile):
+    an = scan['asng'] * scan['nsng']
+    rs = torch.where(an.abs() < 1e-6, torch.zeros_like(an), scan['rsng'] / an)
+    out = []
+    for t in (0, tile):
+        br = batch.BatchRecon(params, replicates, rs, an, device=cuda_device, bs=bs, tile=t)
+        br.run(niter=1, use_graph=False)
+        out.append(br.images())
+        br.geom.check()
+    rl2 = (torch.linalg.vector_norm(out[1] - out[0]) / torch.linalg.vector_norm(out[0])).item()
+    assert rl2 <= 1e-5, f'bs {bs} tile {tile}: relative L2 {rl2:.3e}'
+
+
+def test_autotune_picks_a_valid_shape(params, scan, replicates, cuda_device, tmp_path,
+                                      monkeypatch):
+    monkeypatch.setenv('NIPET_B200_CACHE', str(tmp_path))
+    batch._TUNE_CACHE.clear()
     an = scan['asng'] * scan['nsng']
     rs = torch.where(an.abs() < 1e-6, torch.zeros_like(an), scan['rsng'] / an)
     br = batch.BatchRecon(params, replicates, rs, an, device=cuda_device)
-    assert br.bs in (1, 2, 4)
+    assert br.bs in (1, 2, 4) and br.tile in batch.TILES
+    assert (tmp_path / 'autotune.json').exists()
