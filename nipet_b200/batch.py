@@ -212,11 +212,14 @@ def autotune(rec: BatchRecon, candidates=None, repeats: int = 2):
             best, best_t = (bs, tile), t
     rec.geom.check()
     _TUNE_CACHE[key] = best
-    try:
-        os.makedirs(os.path.dirname(_cache_file()), exist_ok=True)
+    try:  # atomic replace: several processes (one per GPU) may tune at once
+        path = _cache_file()
+        os.makedirs(os.path.dirname(path), exist_ok=True)
         disk[key] = list(best)
-        with open(_cache_file(), 'w') as f:
+        tmp = f'{path}.{os.getpid()}.tmp'
+        with open(tmp, 'w') as f:
             json.dump(disk, f, indent=1)
+        os.replace(tmp, path)
     except Exception:
         pass
     rec.bs, rec.tile = best

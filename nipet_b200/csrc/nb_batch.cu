@@ -528,19 +528,43 @@ __global__ void k_from_batch(float *__restrict__ dst, const float *__restrict__ 
 }
 
 // img = msk ? img * (|sens| < 1e-6 ? 0 : bimg / sens) : 0; bimg = 0  (recon.cu:493-496),
-// sens and msk shared by the BS images of a group
+// sens and msk shared by the BS images of a group: one thread per voxel of a group moves
+// the group's BS values with one vector access (blockIdx.y strides over the groups)
+template <int BS> struct VecF;
+template <> struct VecF<1> { using T = float; };
+template <> struct VecF<2> { using T = float2; };
+template <> struct VecF<4> { using T = float4; };
+
+template <int BS>
 __global__ void k_update_batch(float *__restrict__ img, float *__restrict__ bimg,
                                const float *__restrict__ sens, const uint8_t *__restrict__ msk,
-                               int ngroups, int bs) {
+                               int ngroups) {
+  using V = typename VecF<BS>::T;
   const size_t nvox = (size_t)NB_NCOL * NB_COLW;
-  const size_t n = (size_t)ngroups * nvox * bs;
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
-       t += (size_t)gridDim.x * blockDim.x) {
-    const size_t v = (t / bs) % nvox;
-    const float s = sens[v];
-    const float q = (s > -0.000001f && s < 0.000001f) ? 0.f : __fdiv_rn(bimg[t], s);
-    img[t] = msk[v] ? img[t] * q : 0.f;
-    bimg[t] = 0.f;
+  for (int grp = blockIdx.y; grp < ngroups; grp += gridDim.y) {
+    V *gi = reinterpret_cast<V *>(img + (size_t)grp * nvox * BS);
+    V *gb = reinterpret_cast<V *>(bimg + (size_t)grp * nvox * BS);
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < nvox;
+         v += (size_t)gridDim.x * blockDim.x) {
+      const float s = sens[v];
+      const bool keep = msk[v] != 0;
+      const bool zero_s = s > -0.000001f && s < 0.000001f;
+      V x = gi[v];
+      const V b = gb[v];
+      float *xp = reinterpret_cast<float *>(&x);
+      const float *bp = reinterpret_cast<const float *>(&b);
+#pragma unroll
+      for (int k = 0; k < BS; k++) {
+        const float q = zero_s ? 0.f : __fdiv_rn(bp[k], s);
+        xp[k] = keep ? xp[k] * q : 0.f;
+      }
+      gi[v] = x;
+      V z;
+      float *zp = reinterpret_cast<float *>(&z);
+#pragma unroll
+      for (int k = 0; k < BS; k++) zp[k] = 0.f;
+      gb[v] = z;
+    }
   }
 }
 
@@ -643,7 +667,13 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   }
 #undef NB_TILES
   if (st) return st;
-  k_update_batch<<<g->nsm * 16, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups, bs);
+  const dim3 ugrid(g->nsm * 4, ngroups < 16 ? ngroups : 16);
+  if (bs == 4)
+    k_update_batch<4><<<ugrid, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups);
+  else if (bs == 2)
+    k_update_batch<2><<<ugrid, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups);
+  else
+    k_update_batch<1><<<ugrid, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }
