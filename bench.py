@@ -396,6 +396,19 @@ def run_batch(args, ws, rank, dev):
     peak, peak_kind = _peaks()
     tr8 = _traffic('osem_batch_8img')
     traffic = None if tr8 is None else tr8 * nrep / 8.0
+    # the on-chip bound: shared-memory wavefronts of one launch (ncu count of the 8-image
+    # capture, scaled by images) over the live launch time, against one wavefront per
+    # cycle per SM at the sampled clock
+    wf8 = _traffic('osem_batch_8img_smem_wavefronts')
+    onchip = None
+    if wf8:
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+        ach = wf8 * nrep / 8.0 / (t_it / len(br.subs))
+        onchip = {'bound': 'shared-memory pipe', 'unit': 'wavefronts/s', 'achieved': ach,
+                  'peak': nsm * mhz * 1e6, 'frac': ach / (nsm * mhz * 1e6),
+                  'wavefronts_per_launch': wf8 * nrep / 8.0,
+                  'peak_basis': f'1 wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz'}
 
     # e2e through the public batch API: pinned host prompts -> device, reconstruction,
     # voxel-wise mean/std images back to the host
@@ -447,7 +460,11 @@ def run_batch(args, ws, rank, dev):
                      'kernel': f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk, '
                                f'tile {br.tile})',
                      'peak_kind': peak_kind, 'bytes_per_launch_avg': bytes_iter / len(br.subs),
-                     'launch_ms_avg': t_it * 1e3 / len(br.subs)},
+                     'launch_ms_avg': t_it * 1e3 / len(br.subs),
+                     'note': 'achieved counts 4 B per Siddon voxel read/update as if from HBM; '
+                             'the kernel stages image columns in shared memory and reuses each '
+                             'about 35 times, so its bound is on-chip (see onchip)',
+                     'onchip': onchip},
         'config': {'workload': f'batched bootstrap OSEM, {nrep} replicates '
                                f'({nrep - nlow} at 3e7, {nlow} at 3e6 counts), span-11 '
                                f'837x252x344, 320x320x127 f32, 4 it x 14 subsets + '
