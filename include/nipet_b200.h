@@ -142,6 +142,18 @@ int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens1
  * to and from that layout. */
 int nb_to_batch(float *dst, const float *src, int nrep, int bs, void *stream);
 int nb_from_batch(float *dst, const float *src, int nrep, int bs, void *stream);
+
+/* Forward and back projection of nrep images in the batched layout, one walk of the
+ * geometry per bs images -- what gpu_fprj / gpu_bprj (prjf.cu:209-320, prjb.cu:190-308) do
+ * for one image per call.  Used by the differentiable projector for image batches.
+ *   nb_fprj_batch: sino dev [nrep][nprj][nsinos] float, overwritten (att = 0: emission)
+ *   nb_bprj_batch: bimg dev batched layout, the back projection of sino is ADDED (zero it
+ *                  first); sino dev [nrep][nprj][nsinos]
+ *   subs dev [nprj] LOR indices, or NULL with nprj = 68516. */
+int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep, int bs, int span,
+                  const int32_t *subs, int nprj, void *stream);
+int nb_bprj_batch(nb_geom *g, float *bimg, const float *sino, int nrep, int bs, int span,
+                  const int32_t *subs, int nprj, void *stream);
 int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens128,
                          const uint8_t *msk128, const uint16_t *psng, const float *rs,
                          const float *rscale, int nrep, int bs, int tile, int span,

@@ -49,6 +49,8 @@ SIGNATURES = {
     'nb_to_batch': ([P, P, I, I, P], I),
     'nb_from_batch': ([P, P, I, I, P], I),
     'nb_osem_batch_subset': ([P, P, P, P, P, P, P, P, I, I, I, I, P, I, P], I),
+    'nb_fprj_batch': ([P, P, P, I, I, I, P, I, P], I),
+    'nb_bprj_batch': ([P, P, P, I, I, I, P, I, P], I),
     'nb_osem_rs': ([P, P, P, P, P, C.c_size_t, P], I),
     'nb_osem_subset': ([P, P, P, P, P, P, P, P, I, P], I),
     'nb_lm_plan': ([P, C.c_int64, I, I, I, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I),

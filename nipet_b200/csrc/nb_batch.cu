@@ -40,9 +40,24 @@ struct BatchArgs {
   const uint16_t *psng;    // [nrep][naw][nout]
   const float *rs;         // [naw][nout] (r+s)/(an), scaled per replicate by rscale
   const float *rscale;     // [nrep]
+  float *sino_out;         // forward mode: [nrep][nprj][nout]
+  const float *sino_in;    // backward mode: [nrep][nprj][nout]
   int fxbits;
   int *err;
 };
+
+// kernel modes: the fused OSEM sub-iteration (forward, ratio, backward), a forward
+// projection only (sinogram rows out) and a back projection only (sinogram rows in)
+enum { BMODE_OSEM = 0, BMODE_FWD = 1, BMODE_BWD = 2 };
+
+// a job (LOR, image group) runs nch chunks of the LOR's columns per pass: two passes
+// (forward, then backward) in OSEM mode, one otherwise
+template <int MODE> __device__ __forceinline__ bool bphase_load(int c, int nch) {
+  return MODE == BMODE_OSEM ? c < nch : MODE == BMODE_FWD;
+}
+template <int MODE> __device__ __forceinline__ int bphase_chunk(int c, int nch) {
+  return (MODE == BMODE_OSEM && c >= nch) ? c - nch : c;
+}
 
 // shared-memory layout; every region starts on a 128-byte boundary (the mbarriers in the
 // misc region need 8-byte, the vector/TMA accesses 16-byte alignment)
@@ -88,8 +103,9 @@ __device__ __forceinline__ void bjob_load(const BatchArgs &a, int q, BJob &J) {
   J.nch = J.n > 0 ? (J.n + CH - 1) / CH : 1;
 }
 
-template <int CH> __device__ __forceinline__ void bjob_next(const BatchArgs &a, BJob &J, int &q) {
-  if (++J.c >= 2 * J.nch) {
+template <int CH, int MODE>
+__device__ __forceinline__ void bjob_next(const BatchArgs &a, BJob &J, int &q) {
+  if (++J.c >= (MODE == BMODE_OSEM ? 2 : 1) * J.nch) {
     q += gridDim.x;
     bjob_load<CH>(a, q, J);
   }
@@ -267,7 +283,7 @@ __device__ __forceinline__ void bwalk(BRay<BS, RPT> &S, const void *chunk, const
   for (int r = 0; r < RPT; r++) S.zo[r] = ((int)(cur[r] - sb) - n * (int)colb) << LG;
 }
 
-template <int BS, int CH, int NOUT, int NT, int RPT>
+template <int BS, int CH, int NOUT, int NT, int RPT, int MODE>
 __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   using L = BSmem<BS, CH>;
@@ -307,13 +323,13 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     BJob P = J;
     int qP = blockIdx.x;
     for (int k = 0; k < 2 && P.valid; k++) {
-      const bool ld = P.c < P.nch;
-      const int chunk = ld ? P.c : P.c - P.nch;
+      const bool ld = bphase_load<MODE>(P.c, P.nch);
+      const int chunk = bphase_chunk<MODE>(P.c, P.nch);
       if (ld)
         bissue_load<BS, CH>(a, P, chunk, fbuf + (size_t)k * CH * COLF, tnbuf + k * CH, &bars[k]);
       else
         bload_tn<CH>(a, P, chunk, tnbuf + k * CH);
-      bjob_next<CH>(a, P, qP);
+      bjob_next<CH, MODE>(a, P, qP);
     }
     __syncwarp();
     if (tid == 0) {
@@ -331,13 +347,21 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
     float *fb = fbuf + (size_t)b * CH * COLF;
     int *ib = ibuf + (size_t)b * CH * COLF;
     float *tb = tnbuf + b * CH;
-    const bool load = J.c < J.nch;
-    const int chunk = load ? J.c : J.c - J.nch;
+    const bool load = bphase_load<MODE>(J.c, J.nch);
+    const int chunk = bphase_chunk<MODE>(J.c, J.nch);
     const int n = max(0, min(CH, J.n - chunk * CH));
 
     if (chunk == 0) {
       const float4 h = a.hdr[J.lor];
       brays_init<BS, NT, RPT>(a, h, S);
+      if (MODE == BMODE_BWD) {  // the rows to back project take the place of the ratio
+        for (int x = tid; x < NOUT * BS; x += NT) {
+          const int o = x / BS, k = x - o * BS;
+          const int rep = J.g * BS + k;
+          rat[x] = rep < a.nrep ? a.sino_in[((size_t)rep * a.nprj + J.p) * NOUT + o] : 0.f;
+        }
+        __syncthreads();
+      }
       if (!load) {
         // one fixed-point scale per image: images of one group can differ in count level
         // by orders of magnitude, and a shared scale would quantise the quieter ones'
@@ -442,6 +466,10 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
           v = vals[a.bin1[o] * BS + k];
         }
         const int rep = J.g * BS + k;
+        if (MODE == BMODE_FWD) {
+          if (rep < a.nrep) a.sino_out[((size_t)rep * a.nprj + J.p) * NOUT + o] = v;
+          continue;
+        }
         float rr = 0.f;
         if (rep < a.nrep) {
           const size_t gi = (size_t)J.lor * NOUT + o;
@@ -467,15 +495,15 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
       BJob P = *sP;
       int qP = *sqP;
       if (P.valid) {
-        const bool ld = P.c < P.nch;
-        const int pch = ld ? P.c : P.c - P.nch;
+        const bool ld = bphase_load<MODE>(P.c, P.nch);
+        const int pch = bphase_chunk<MODE>(P.c, P.nch);
         if (ld) {
           nb_bulk_wait_read<0>();
           bissue_load<BS, CH>(a, P, pch, fb, tb, &bars[b]);
         } else {
           bload_tn<CH>(a, P, pch, tb);
         }
-        bjob_next<CH>(a, P, qP);
+        bjob_next<CH, MODE>(a, P, qP);
       }
       __syncwarp();
       if (tid == 0) {
@@ -483,7 +511,7 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
         *sqP = qP;
       }
     }
-    bjob_next<CH>(a, J, qJ);
+    bjob_next<CH, MODE>(a, J, qJ);
     ++j;
   }
   if (*sflag && tid == 0) nb_set_error(a.err, NB_DEVERR_MBAR_TIMEOUT);
@@ -568,7 +596,7 @@ __global__ void k_update_batch(float *__restrict__ img, float *__restrict__ bimg
   }
 }
 
-template <int BS, int CH, int NOUT, int NT, int RPT>
+template <int BS, int CH, int NOUT, int NT, int RPT, int MODE = nbb::BMODE_OSEM>
 int launch_batch(nb_geom *g, const nbb::BatchArgs &a, cudaStream_t s) {
   static_assert(NT * RPT >= NB_NRAYS, "not enough ray slots");
   static_assert(nbb::BSmem<BS, CH>::template misc_off<NOUT>() % 128 == 0, "misaligned barriers");
@@ -576,16 +604,47 @@ int launch_batch(nb_geom *g, const nbb::BatchArgs &a, cudaStream_t s) {
   const size_t smem = nbb::BSmem<BS, CH>::template total<NOUT>();
   static bool set[64] = {false};
   if (!set[g->device & 63]) {
-    NB_CUDA(cudaFuncSetAttribute(nbb::k_osem_batch<BS, CH, NOUT, NT, RPT>,
+    NB_CUDA(cudaFuncSetAttribute(nbb::k_osem_batch<BS, CH, NOUT, NT, RPT, MODE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     set[g->device & 63] = true;
   }
   const long jobs = (long)a.nprj * a.ngroups;
   const int grid = jobs < g->nsm ? (int)jobs : g->nsm;
   if (grid <= 0) return NB_OK;
-  nbb::k_osem_batch<BS, CH, NOUT, NT, RPT><<<grid, NT, smem, s>>>(a);
+  nbb::k_osem_batch<BS, CH, NOUT, NT, RPT, MODE><<<grid, NT, smem, s>>>(a);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
+}
+
+// geometry fields of the batched kernels' arguments
+void batch_geometry(nb_geom *g, nbb::BatchArgs &a, int nrep, int bs, int span,
+                    const int32_t *subs, int nprj) {
+  a.scol = g->d_scol;
+  a.st = g->d_st;
+  a.hdr = g->d_hdr;
+  a.rays = g->d_rays;
+  a.bin11 = g->d_bin11;
+  a.bin1 = g->d_bin1;
+  a.subs = subs;
+  a.nprj = nprj;
+  a.naw = g->naw;
+  a.span = span;
+  a.ngroups = (nrep + bs - 1) / bs;
+  a.nrep = nrep;
+  a.fxbits = g->fxbits;
+  a.err = g->d_err;
+}
+
+// forward (MODE_FWD) or back (MODE_BWD) projection of nrep batched images, default tile
+template <int MODE> int launch_batch_prj(nb_geom *g, const nbb::BatchArgs &a, int bs, int span,
+                                         cudaStream_t s) {
+  if (span == 11) {
+    if (bs == 4) return launch_batch<4, 16, NB_NSN11, 1024, 4, MODE>(g, a, s);
+    if (bs == 2) return launch_batch<2, 32, NB_NSN11, 1024, 4, MODE>(g, a, s);
+    return launch_batch<1, 64, NB_NSN11, 1024, 4, MODE>(g, a, s);
+  }
+  if (bs == 2) return launch_batch<2, 32, NB_NSN1, 1024, 4, MODE>(g, a, s);
+  return launch_batch<1, 64, NB_NSN1, 1024, 4, MODE>(g, a, s);
 }
 
 }  // namespace
@@ -626,25 +685,12 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   cudaStream_t s = (cudaStream_t)stream;
   const int ngroups = (nrep + bs - 1) / bs;
   nbb::BatchArgs a{};
-  a.scol = g->d_scol;
-  a.st = g->d_st;
-  a.hdr = g->d_hdr;
-  a.rays = g->d_rays;
-  a.bin11 = g->d_bin11;
-  a.bin1 = g->d_bin1;
-  a.subs = subs;
-  a.nprj = nprj;
-  a.naw = g->naw;
-  a.span = span;
-  a.ngroups = ngroups;
-  a.nrep = nrep;
+  batch_geometry(g, a, nrep, bs, span, subs, nprj);
   a.img = img;
   a.bimg = bimg;
   a.psng = psng;
   a.rs = rs;
   a.rscale = rscale;
-  a.fxbits = g->fxbits;
-  a.err = g->d_err;
   // kernel shape per (span, bs, tile): columns per staged chunk (CH), threads (NT) and
   // rays per thread (RPT); CH * 128 * bs floats per chunk buffer
 #define NB_TILES(BS, CH, NOUT)                                                            \
@@ -676,4 +722,38 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
     k_update_batch<1><<<ugrid, 256, 0, s>>>(img, bimg, sens128, msk128, ngroups);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
+}
+
+extern "C" int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep, int bs,
+                             int span, const int32_t *subs, int nprj, void *stream) {
+  NB_REQUIRE(g != nullptr, "nb_fprj_batch: NULL geometry handle");
+  NB_REQUIRE(sino && img, "nb_fprj_batch: NULL argument");
+  NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_fprj_batch: nrep out of range");
+  NB_REQUIRE(span == 11 || span == 1, "nb_fprj_batch: span must be 1 or 11");
+  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
+             "nb_fprj_batch: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(nprj > 0 && (subs != nullptr || nprj == g->naw), "nb_fprj_batch: bad subset");
+  NB_CUDA(cudaSetDevice(g->device));
+  nbb::BatchArgs a{};
+  batch_geometry(g, a, nrep, bs, span, subs, nprj);
+  a.img = img;
+  a.sino_out = sino;
+  return launch_batch_prj<nbb::BMODE_FWD>(g, a, bs, span, (cudaStream_t)stream);
+}
+
+extern "C" int nb_bprj_batch(nb_geom *g, float *bimg, const float *sino, int nrep, int bs,
+                             int span, const int32_t *subs, int nprj, void *stream) {
+  NB_REQUIRE(g != nullptr, "nb_bprj_batch: NULL geometry handle");
+  NB_REQUIRE(sino && bimg, "nb_bprj_batch: NULL argument");
+  NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_bprj_batch: nrep out of range");
+  NB_REQUIRE(span == 11 || span == 1, "nb_bprj_batch: span must be 1 or 11");
+  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
+             "nb_bprj_batch: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(nprj > 0 && (subs != nullptr || nprj == g->naw), "nb_bprj_batch: bad subset");
+  NB_CUDA(cudaSetDevice(g->device));
+  nbb::BatchArgs a{};
+  batch_geometry(g, a, nrep, bs, span, subs, nprj);
+  a.bimg = bimg;
+  a.sino_in = sino;
+  return launch_batch_prj<nbb::BMODE_BWD>(g, a, bs, span, (cudaStream_t)stream);
 }

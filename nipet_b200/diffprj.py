@@ -26,6 +26,7 @@ __all__ = ['MMRProjector', 'ForwardProjection', 'poisson_nll']
 
 NAW = 68516
 IMG_SHAPE = (320, 320, 127)
+COL128 = 320 * 320 * 128
 
 
 class MMRProjector:
@@ -74,21 +75,46 @@ class MMRProjector:
     def _subs_ptr(self):
         return dev_ptr(self.subs) if self.subs is not None else None
 
+    def _width(self, nimg: int) -> int:
+        """Images per walk of the geometry for a batch of nimg (1, 2 or, at span 11, 4)."""
+        if nimg >= 4 and self.span == 11:
+            return 4
+        return 2 if nimg >= 2 else 1
+
     def project(self, x: torch.Tensor, att: int = 0) -> torch.Tensor:
-        """A x for [B, 320, 320, 127] x (att=1: exp(-A x), the attenuation factors)."""
-        out = torch.empty((x.shape[0], self.nprj, self.nsn), device=self.device)
+        """A x for [B, 320, 320, 127] x (att=1: exp(-A x), the attenuation factors).  Batches
+        of two or more emission images share each walk of the geometry (nb_fprj_batch)."""
+        B = x.shape[0]
+        out = torch.empty((B, self.nprj, self.nsn), device=self.device)
         st = stream_ptr(self.device)
-        for b in range(x.shape[0]):
+        if att == 0 and B >= 2:
+            bs = self._width(B)
+            xb = torch.empty(((B + bs - 1) // bs) * bs * COL128, device=self.device)
+            _lib.check(self.lib.nb_to_batch(dev_ptr(xb), dev_ptr(x), B, bs, st))
+            _lib.check(self.lib.nb_fprj_batch(self.geom.handle, dev_ptr(out), dev_ptr(xb), B,
+                                              bs, self.span, self._subs_ptr(), self.nprj, st))
+            self.launches += 2
+            return out
+        for b in range(B):
             _lib.check(self.lib.nb_fprj(self.geom.handle, dev_ptr(out[b]), dev_ptr(x[b]),
                                         self._subs_ptr(), self.nprj, self.span, att, st))
             self.launches += 2
         return out
 
     def backproject(self, s: torch.Tensor) -> torch.Tensor:
-        """A^T s for [B, nprj, nsinos] s."""
-        out = torch.empty((s.shape[0],) + IMG_SHAPE, device=self.device)
+        """A^T s for [B, nprj, nsinos] s (batches of two or more: nb_bprj_batch)."""
+        B = s.shape[0]
+        out = torch.empty((B,) + IMG_SHAPE, device=self.device)
         st = stream_ptr(self.device)
-        for b in range(s.shape[0]):
+        if B >= 2:
+            bs = self._width(B)
+            bimg = torch.zeros(((B + bs - 1) // bs) * bs * COL128, device=self.device)
+            _lib.check(self.lib.nb_bprj_batch(self.geom.handle, dev_ptr(bimg), dev_ptr(s), B,
+                                              bs, self.span, self._subs_ptr(), self.nprj, st))
+            _lib.check(self.lib.nb_from_batch(dev_ptr(out), dev_ptr(bimg), B, bs, st))
+            self.launches += 2
+            return out
+        for b in range(B):
             _lib.check(self.lib.nb_bprj(self.geom.handle, dev_ptr(out[b]), dev_ptr(s[b]),
                                         self._subs_ptr(), self.nprj, self.span, st))
             self.launches += 2

@@ -7,7 +7,8 @@ Checks (float32 projections, float64 dot products and log-likelihoods):
   * gradient of the Poisson NLL against central finite differences at 64 random voxels,
     h = 1e-3 relative to the voxel value: relative 1e-2 per voxel (plus 1e-3 of the
     largest gradient as an absolute floor);
-  * a batch of 8 images gives the same gradients as the images one at a time: 1e-6;
+  * a batch of 8 images (batched projector pair) gives the gradients of the images one
+    at a time (single-image projectors): relative L2 1e-5, NLL 1e-6;
   * the Function keeps no tensor between forward and backward (weights recomputed).
 """
 import numpy as np
@@ -123,9 +124,11 @@ def test_batch_of_8_matches_single_images(params, cuda_device, weights_in):
         x1 = xb.detach()[b].clone().requires_grad_(True)
         l1 = diffprj.poisson_nll(prj(x1) + 0.1, y)
         (g1,) = torch.autograd.grad(l1, x1)
-        assert abs(float(l1) - float(loss[b])) <= 1e-12 * abs(float(l1))
+        # the batch shares each walk of the geometry over 4 images (nb_fprj_batch /
+        # nb_bprj_batch); one image goes through nb_fprj / nb_bprj: equal to rounding
+        assert abs(float(l1) - float(loss[b])) <= 1e-6 * abs(float(l1))
         rl2 = float(torch.linalg.vector_norm(g1 - gb[b]) / torch.linalg.vector_norm(g1))
-        assert rl2 <= 1e-6, rl2
+        assert rl2 <= 1e-5, rl2
     prj.check()
 
 
