@@ -178,6 +178,12 @@ __device__ __forceinline__ float oblique_s(const nb_ray &R, float atn) {
   return __fsqrt_rn(__fmaf_rn(az_atn, az_atn, 1.0f));
 }
 
+// BS floats as one vector type (16-, 8- or 4-byte accesses)
+template <int BS> struct VecF;
+template <> struct VecF<1> { using T = float; };
+template <> struct VecF<2> { using T = float2; };
+template <> struct VecF<4> { using T = float4; };
+
 template <int BS> struct VecT;
 template <> struct VecT<1> { static __device__ __forceinline__ void ld(uint32_t a, float *v) { v[0] = lds_f32(a); } };
 template <> struct VecT<2> {
@@ -426,15 +432,20 @@ __global__ void __launch_bounds__(NT, 1) k_osem_batch(const BatchArgs a) {
       // int32 [col][BS][128] -> float staging [col][128][BS] (the image layout the bulk
       // reduce adds into), zeroing the accumulators; slot 127 (padding) is not written back
       const int nv = n * NB_COLW;
+      float inv[BS];
+#pragma unroll
+      for (int k = 0; k < BS; k++) inv[k] = sinv[k];
       for (int x = tid; x < nv; x += NT) {
         const int c = x >> 7, slot = x & 127;
+        typename VecF<BS>::T vout;  // the slot's BS values, one vector store
+        float *vo = reinterpret_cast<float *>(&vout);
 #pragma unroll
         for (int k = 0; k < BS; k++) {
           const int src = c * COLF + k * NB_COLW + slot;
-          const int q = ib[src];
-          fb[c * COLF + slot * BS + k] = slot == 127 ? 0.f : (float)q * sinv[k];
+          vo[k] = slot == 127 ? 0.f : (float)ib[src] * inv[k];
           ib[src] = 0;
         }
+        *reinterpret_cast<typename VecF<BS>::T *>(fb + c * COLF + slot * BS) = vout;
       }
       nb_fence_proxy_async_smem();
     }
@@ -558,16 +569,12 @@ __global__ void k_from_batch(float *__restrict__ dst, const float *__restrict__ 
 // img = msk ? img * (|sens| < 1e-6 ? 0 : bimg / sens) : 0; bimg = 0  (recon.cu:493-496),
 // sens and msk shared by the BS images of a group: one thread per voxel of a group moves
 // the group's BS values with one vector access (blockIdx.y strides over the groups)
-template <int BS> struct VecF;
-template <> struct VecF<1> { using T = float; };
-template <> struct VecF<2> { using T = float2; };
-template <> struct VecF<4> { using T = float4; };
 
 template <int BS>
 __global__ void k_update_batch(float *__restrict__ img, float *__restrict__ bimg,
                                const float *__restrict__ sens, const uint8_t *__restrict__ msk,
                                int ngroups) {
-  using V = typename VecF<BS>::T;
+  using V = typename nbb::VecF<BS>::T;
   const size_t nvox = (size_t)NB_NCOL * NB_COLW;
   for (int grp = blockIdx.y; grp < ngroups; grp += gridDim.y) {
     V *gi = reinterpret_cast<V *>(img + (size_t)grp * nvox * BS);
