@@ -10,7 +10,8 @@
 // is shared by the Bs replicates of a ray.  A persistent CTA takes (LOR, group) jobs; per
 // job it runs the forward pass of the LOR for the Bs images, forms the Bs ratio rows
 // y_b / (Ax_b + c_b (r+s)/(an)) and back projects them, exactly as the single-image
-// kernel (nb_project.cuh) does for one image.
+// kernel (nb_project.cuh) does for one image.  The same kernel in forward-only and
+// backward-only mode is the batched projector pair (nb_fprj_batch / nb_bprj_batch).
 #include <math.h>
 
 #include "nb_axial.cuh"
