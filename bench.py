@@ -653,41 +653,82 @@ def run_dynamic(args, ws, rank, dev):
 # list-mode histogram workload
 # ---------------------------------------------------------------------------------------
 def run_hist(args, ws, rank, dev):
+    """One step = every output of the list-mode configuration from one stream: the span-11
+    and span-1 histograms (prompt/delayed sinograms, SSRB, head curves, fan sums, views,
+    singles) and 10 Poisson bootstrap replicates at span 11 (one launch)."""
     import torch
     from nipet_b200 import geometry, mmr_lmproc, phantoms
     params = geometry.get_mmrparams()
-    Cnt = dict(params['Cnt'], SPN=11, BTP=0, DEVID=dev.index)
+    Cnt11 = dict(params['Cnt'], SPN=11, BTP=0, DEVID=dev.index)
+    Cnt1 = dict(Cnt11, SPN=1)
+    CntB = dict(Cnt11, BTP=2, BTPRT=1.0)
+    nboot = 10
     lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=rank,
                                  device=dev)
     lm_host = lm.cpu().numpy()
     pl = mmr_lmproc.plan(lm_host)
+    calls = [(Cnt11, 1), (Cnt1, 1), (CntB, nboot)]
+
+    def step(record=None):
+        for i, (C, nrep) in enumerate(calls):
+            if record is not None:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+            r = mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], C, pl=pl,
+                                       nrep=nrep, seed=rank + 7, unpack=True)
+            if record is not None:
+                e1.record()
+                record.append((i, e0, e1))
+            del r
+
     for _ in range(args.warmup):
-        mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], Cnt, pl=pl, unpack=False)
+        step()
     torch.cuda.synchronize(dev)
-    times = []
+    times, ev = [], []
     clk = Clocks(dev.index) if rank == 0 else None
     for _ in range(args.steps):
         _barrier(ws, dev)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], Cnt, pl=pl, unpack=True)
+        step(ev)
         t1.record()
         _barrier(ws, dev)
         times.append(t0.elapsed_time(t1) / 1e3)
     clocks = clk.stop() if clk else None
     t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
-    nev = int(lm.numel())
-    # e2e: pinned host words -> plan -> device -> histogram -> pinned host sinograms
+    # roofline (per histogram produced): 4 B per stream word read, 8 B per counter
+    # read-modify-write (one sinogram counter per event), 4 B per packed output bin
+    nwords = int(lm.numel())
+    ntag = int(pl['nitag'])
+    nbins = {11: 72557856, 1: 354033792}
+    byt = {i: nrep * (4 * nwords + 8 * (nwords - ntag) + 4 * nbins[C['SPN']])
+           for i, (C, nrep) in enumerate(calls)}
+    dur = sum(a.elapsed_time(b) for _, a, b in ev) / 1e3
+    achieved = sum(byt[i] for i, _, _ in ev) / dur / 1e9
+    peak, peak_kind = _peaks()
+    tr = _traffic('hist_20M_words')
+    roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+            'frac': achieved / peak, 'peak_kind': peak_kind,
+            'traffic': None if tr is None else tr * nwords / 20_020_000 * (2 + nboot) / 3,
+            'kernel': 'k_hist (+ unpack), span 11, span 1, 10 bootstrap replicates'}
+    nev = nwords
+    # e2e: pinned host words -> plan -> device -> every output's sinograms in pinned host
+    # memory (span 11, span 1, the bootstrap replicates)
     lm_pin = torch.from_numpy(lm_host).pin_memory()
-    psn_h = torch.empty((837, 252, 344), dtype=torch.uint16).pin_memory()
-    dsn_h = torch.empty_like(psn_h).pin_memory()
+    outs = {i: (torch.empty((nrep, nbins[C['SPN']]), dtype=torch.uint16).pin_memory(),
+                torch.empty((nrep, nbins[C['SPN']]), dtype=torch.uint16).pin_memory())
+            for i, (C, nrep) in enumerate(calls)}
 
     def e2e_step():
         p2 = mmr_lmproc.plan(lm_pin.numpy())
-        r = mmr_lmproc.hist_stream(lm_pin, params['txLUT'], params['axLUT'], Cnt, pl=p2)
-        psn_h.copy_(r['psn'])
-        dsn_h.copy_(r['dsn'])
+        for i, (C, nrep) in enumerate(calls):
+            r = mmr_lmproc.hist_stream(lm_pin, params['txLUT'], params['axLUT'], C, pl=p2,
+                                       nrep=nrep, seed=rank + 7)
+            outs[i][0].copy_(r['psn'].reshape(nrep, -1))
+            outs[i][1].copy_(r['dsn'].reshape(nrep, -1))
+            del r
         torch.cuda.synchronize(dev)
 
     e2e_step()
@@ -700,11 +741,13 @@ def run_hist(args, ws, rank, dev):
     te = _max_over_ranks(float(np.mean(et)), ws, dev)
     res = {'ms_per_step': t_step * 1e3, 'value': ws * nev / t_step,
            'e2e': {'value': ws * nev / te, 'unit': 'events/s', 'h2d_bytes_per_step': nev * 4,
-                   'd2h_bytes_per_step': 2 * 2 * 72557856},
-           'clocks': clocks, 'gpu_launches': 3,
-           'roofline': None,
-           'config': {'workload': f'list-mode histogram span-11, {nev} words over '
-                                  f'{args.duration} s', 'global_batch': ws,
+                   'd2h_bytes_per_step': sum(2 * 2 * nrep * nbins[C['SPN']]
+                                             for C, nrep in calls)},
+           'clocks': clocks, 'gpu_launches': sum(1 + nrep for _, nrep in calls),
+           'roofline': roof,
+           'config': {'workload': f'list-mode histogram of {nev} words over {args.duration} s: '
+                                  f'span 11, span 1 and {nboot} Poisson bootstrap replicates '
+                                  '(span 11) per step', 'global_batch': ws,
                       'parallelism': f'replicas x{ws}', 'l2': 'input larger than L2'}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         res['cpu_baseline'] = cpu_hist_sample(lm_host, params)
@@ -769,10 +812,14 @@ def run_reference(args):
             for _ in range(args.warmup + args.steps):
                 t = time.perf_counter()
                 ref.hist(params, path, span=11)
+                ref.hist(params, path, span=1)
+                for _ in range(10):  # the reference draws one bootstrap replicate per call
+                    ref.hist(params, path, span=11, btp=2, btprt=1.0)
                 ts.append(time.perf_counter() - t)
         v = lm.size / float(np.mean(ts[args.warmup:]))
         sample = (f'{lm.size} words over {args.duration} s per step through the reference CUDA '
-                  'build (lmproc: file read, chunking, gpu_hst, span 11) on this GPU')
+                  'build (lmproc: file read, chunking, gpu_hst): span 11, span 1 and 10 '
+                  'Poisson bootstrap replicates (span 11), on this GPU')
         line.update({'value': v, 'n_gpus': 1, 'ms_per_step': lm.size / v * 1e3,
                      'dtype': 'u32',
                      'config': {'workload': 'hist', 'implementation':

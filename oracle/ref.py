@@ -37,7 +37,7 @@ def load():
         lib.ref_osem.argtypes = [P, P, P, P, P, P, P, P, I, I, P, P, P, P, P, P, I, I, P]
         lib.ref_tables.argtypes = [P, P, P, P, I]
         lib.ref_lminfo.argtypes = [C.c_char_p, I, P]
-        lib.ref_hist.argtypes = [C.c_char_p, I, I, I] + [P] * 13 + [P, P, P]
+        lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
                   lib.ref_hist):
             f.restype = I
@@ -124,8 +124,9 @@ def tables(params):
     return tt, tv
 
 
-def hist(params, path, span=11, t0=0, t1=0):
-    """Reference lmproc (no bootstrap) on a list-mode file: returns a dict of host arrays
+def hist(params, path, span=11, t0=0, t1=0, btp=0, btprt=1.0):
+    """Reference lmproc on a list-mode file (btp: 0 none, 1/2 the reference's clock-seeded
+    bootstrap, not reproducible): returns a dict of host arrays
     (`psn`, `dsn`, `ssr`, `pvs`, `phc`, `dhc`, `mss`, `fan`, `bck`, `psum`, `dsum`) and the
     time of the call in ms."""
     lib = load()
@@ -145,7 +146,7 @@ def hist(params, path, span=11, t0=0, t1=0):
     s16 = lambda a: np.ascontiguousarray(a, np.int16)  # noqa: E731
     luts = (s16(tx['s2cF']), s16(ax['sn1_rno']), s16(ax['sn1_sn11']), s16(ax['sn1_ssrb']))
     psm, dsm, ms = C.c_ulonglong(), C.c_ulonglong(), C.c_float()
-    _check(lib.ref_hist(bpath, t0, t1, span, *[_p(a) for a in luts],
+    _check(lib.ref_hist(bpath, t0, t1, span, int(btp), float(btprt), *[_p(a) for a in luts],
                         *[_p(out[k]) for k in ('psn', 'dsn', 'ssr', 'pvs', 'phc', 'dhc', 'mss',
                                                'fan', 'bck')],
                         C.byref(psm), C.byref(dsm), C.byref(ms)), 'hist')

@@ -214,13 +214,15 @@ int ref_lminfo(const char *fname, int bpe, int *nitag) {
   return (int)cudaGetLastError();
 }
 
-// Histogram of a list-mode file by the reference's lmproc (lm/src/lmproc.cu) without
-// bootstrap, as mmr_lmproc.hist calls it (lm_module.cu:174-391): outputs sized by the
+// Histogram of a list-mode file by the reference's lmproc (lm/src/lmproc.cu), as
+// mmr_lmproc.hist calls it (lm_module.cu:174-391); btp 0 (none), 1 or 2 (bootstrap with
+// the reference's clock-seeded curand, btprt the Poisson mean): outputs sized by the
 // caller for nitag time tags -- psn/dsn [tot_bins] uint16, ssr [127*86688], snv [sne],
 // hcp/hcd/mss [nitag], fan [64*504], bck [2*224*nitag].  s2cF [86688][2], sn1_rno
 // [4084][2], sn1_sn11 [4084], sn1_ssrb [4084] (txLUT / axLUT arrays).  *ms: time of
 // the call (file reading included).
-int ref_hist(const char *fname, int tstart, int tstop, int span, const int16_t *s2cF,
+int ref_hist(const char *fname, int tstart, int tstop, int span, int btp, float btprt,
+             const int16_t *s2cF,
              const int16_t *sn1_rno, const int16_t *sn1_sn11, const int16_t *sn1_ssrb,
              uint16_t *psn, uint16_t *dsn, uint32_t *ssr, uint32_t *snv, uint32_t *hcp,
              uint32_t *hcd, float *mss, uint32_t *fan, uint32_t *bck,
@@ -228,8 +230,8 @@ int ref_hist(const char *fname, int tstart, int tstop, int span, const int16_t *
   Cnst c = make_cnst(span);
   c.BPE = 4;
   c.LMOFF = 0;
-  c.BTP = 0;
-  c.BTPRT = 1.f;
+  c.BTP = (char)btp;
+  c.BTPRT = btprt;
   c.W = NSBINS;
   c.A = NSANGLES;
   c.NSN1 = NSINOS;
