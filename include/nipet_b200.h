@@ -123,6 +123,23 @@ int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens1
                    const uint8_t *msk128, const uint16_t *psng, const float *rs,
                    const int32_t *subs, int nprj, void *stream);
 
+/* Resolution modelling (recon.cu:49-216, the PSF of petprj.osem when krnl[0][0] >= 0).
+ * nb_psf_col128: the reference's separable convolution of one col128 image -- along z
+ *   with krnl row 0, then x with row 1, then y with row 2 (the row order psf_config,
+ *   prj/mmrrec.py:96-155, produces), 17 taps, zeros outside the volume; bit-identical to
+ *   the reference's d_conv.  krnl host [3][17]; dst may equal src; tmp128 dev col128
+ *   scratch distinct from both.
+ * nb_osem_subset_psf: nb_osem_subset with the PSF inside the sub-iteration
+ *   (recon.cu:459-497): forward projection of the convolved image, convolution of the
+ *   back projection before the division by sens128 (which the caller has convolved once,
+ *   recon.cu:437-445).  work128 dev 2 x col128 scratch. */
+int nb_psf_col128(float *dst128, const float *src128, const float *krnl, float *tmp128,
+                  void *stream);
+int nb_osem_subset_psf(nb_geom *g, float *img128, float *bimg128, const float *sens128,
+                       const uint8_t *msk128, const uint16_t *psng, const float *rs,
+                       const int32_t *subs, int nprj, const float *krnl, float *work128,
+                       void *stream);
+
 /* ---- batched OSEM: many images (bootstrap replicates, dynamic frames) per launch --------
  * The reference reconstructs one image per osem() call (recon.cu:318-521); these entry
  * points run one sub-iteration for nrep images that share geometry, attenuation,

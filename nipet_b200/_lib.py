@@ -53,6 +53,8 @@ SIGNATURES = {
     'nb_bprj_batch': ([P, P, P, I, I, I, P, I, P], I),
     'nb_osem_rs': ([P, P, P, P, P, C.c_size_t, P], I),
     'nb_osem_subset': ([P, P, P, P, P, P, P, P, I, P], I),
+    'nb_psf_col128': ([P, P, P, P, P], I),
+    'nb_osem_subset_psf': ([P, P, P, P, P, P, P, P, I, P, P, P], I),
     'nb_lm_plan': ([P, C.c_int64, I, I, I, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I),
                     C.POINTER(I), C.POINTER(I)], I),
     'nb_hist': ([P, C.c_int64, I, P, P, P, I, I, I, I, I, I, C.c_double, C.c_uint64, I, I, P, P,

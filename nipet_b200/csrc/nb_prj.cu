@@ -253,6 +253,43 @@ extern "C" int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const f
   return NB_OK;
 }
 
+extern "C" int nb_psf_col128(float *dst128, const float *src128, const float *krnl,
+                             float *tmp128, void *stream);
+
+// One OSEM sub-iteration with resolution modelling (recon.cu:459-497 with krnl[0] >= 0):
+// the forward projection sees the PSF-convolved image, the back-projected ratio is
+// convolved before the division by the (already convolved) sensitivity.  work128 holds two
+// col128 images of scratch.
+extern "C" int nb_osem_subset_psf(nb_geom *g, float *img128, float *bimg128,
+                                  const float *sens128, const uint8_t *msk128,
+                                  const uint16_t *psng, const float *rs, const int32_t *subs,
+                                  int nprj, const float *krnl, float *work128, void *stream) {
+  int st = check_common(g, nprj, subs, 11);
+  if (st) return st;
+  NB_REQUIRE(img128 && bimg128 && sens128 && msk128 && psng && rs && subs && krnl && work128,
+             "nb_osem_subset_psf: NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  float *rm = work128, *tmp = work128 + NB_IMG_COL128;
+  st = nb_psf_col128(rm, img128, krnl, tmp, stream);
+  if (st) return st;
+  NB_CUDA(cudaMemsetAsync(bimg128, 0, sizeof(float) * NB_IMG_COL128, s));
+  PrjArgs a = base_args(g, subs, nprj, 11);
+  a.img = rm;
+  a.bimg = bimg128;
+  a.psng = psng;
+  a.rs = rs;
+  st = launch_project<MODE_OSEM, CH_BWD>(g, a, s);
+  if (st) return st;
+  st = nb_psf_col128(rm, bimg128, krnl, tmp, stream);  // rm: the convolved back projection
+  if (st) return st;
+  NB_CUDA(cudaMemsetAsync(bimg128, 0, sizeof(float) * NB_IMG_COL128, s));
+  const size_t n4 = NB_IMG_COL128 / 4;
+  k_osem_update<<<g->nsm * 8, 256, 0, s>>>((float4 *)img128, (float4 *)rm,
+                                           (const float4 *)sens128, (const uchar4 *)msk128, n4);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
 extern "C" int nb_geom_count_reads(nb_geom *g, long long *per_lor, long long *reads) {
   NB_REQUIRE(g && reads, "nb_geom_count_reads: NULL argument");
   NB_CUDA(cudaSetDevice(g->device));

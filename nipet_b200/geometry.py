@@ -46,6 +46,7 @@ def get_mmr_constants() -> dict:
         # GPU image (y, x, z) and Siemens image (z, y, x)
         'SZ_IMX': 320, 'SZ_IMY': 320, 'SZ_IMZ': 127,
         'SZ_VOXY': 0.208626, 'SZ_VOXZ': 0.203125,
+        'RSZ_PSF_KRNL': 8,  # PSF kernel radius in voxels (include/def.h:114)
         'SO_IMX': 344, 'SO_IMY': 344, 'SO_IMZ': 127,
         'SO_VXX': 0.208626, 'SO_VXY': 0.208626, 'SO_VXZ': 0.203125,
         'TFOV2': 890.0,

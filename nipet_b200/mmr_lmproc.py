@@ -105,9 +105,12 @@ def hist_stream(lm, txLUT: dict, axLUT: dict, Cnt: dict, t0: int = 0, t1: int = 
             s16(txLUT['s2cF']))
     hp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
     st = stream_ptr(dev)
+    # plan arrays in the dtypes nb_hist reads, held until the call returns
+    atag = np.ascontiguousarray(pl['atag'], dtype=np.int64)
+    e4c = np.ascontiguousarray(pl['ele4chnk'], dtype=np.int32)
+    e4t = np.ascontiguousarray(pl['ele4thrd'], dtype=np.int32)
     _lib.check(_lib.load().nb_hist(
-        dev_ptr(d_lm), d_lm.numel(), pl['nchnk'], hp(np.ascontiguousarray(pl['atag'])),
-        hp(np.ascontiguousarray(pl['ele4chnk'])), hp(np.ascontiguousarray(pl['ele4thrd'])),
+        dev_ptr(d_lm), d_lm.numel(), pl['nchnk'], hp(atag), hp(e4c), hp(e4t),
         pl['toff'], nitag, pl['tstart'], pl['tstop'], span, btp, btprt, int(seed), int(rep0),
         int(nrep), *[hp(a) for a in luts], dev_ptr(out['psino']), dev_ptr(out['ssr']),
         dev_ptr(out['phc']), dev_ptr(out['dhc']), dev_ptr(out['zR']), dev_ptr(out['zM']),

@@ -25,6 +25,54 @@ __all__ = ['get_subsets14', 'subset_table', 'synthetic_scan', 'Recon', 'norm_sin
 NAW = 68516
 
 
+def fwhm2sig(fwhm, voxsize=1.0):
+    """Gaussian sigma (in voxels) of a FWHM (same unit as voxsize) (prj/mmrrec.py:34-35)."""
+    return (fwhm / voxsize) / (2 * (2 * np.log(2)) ** .5)
+
+
+def psf_config(psf, Cnt: dict) -> np.ndarray:
+    """The [3, 2*RSZ_PSF_KRNL+1] separable resolution kernel `petprj.osem` takes, built as
+    the reference's `psf_config` (prj/mmrrec.py:96-155): rows z, x, y (each normalised
+    Gaussian); None switches PSF off (kernel[0, 0] = -1); a scalar FWHM [mm] is isotropic;
+    [x, y, z] FWHMs per axis; a [3, 17] array gives the x, y, z kernels directly.  The
+    measured mMR PSF ('measured') lives in the un-vendored `nimpa` and is not provided."""
+    from numbers import Real
+    R = int(Cnt.get('RSZ_PSF_KRNL', 8))
+
+    def _config(fwhm3, check_len=True):
+        if check_len and (len(fwhm3) != 3 or any(f < 0 for f in fwhm3)):
+            raise ValueError('Incorrect separable kernel FWHM definition')
+        kernel = np.empty((3, 2 * R + 1), dtype=np.float32)
+        for i, f in enumerate(fwhm3):
+            sig = fwhm2sig(f, voxsize=Cnt['SZ_VOXZ' if i == 2 else 'SZ_VOXY'] * 10)
+            x = np.arange(-R, R + 1)
+            kernel[i, :] = np.exp(-0.5 * (x ** 2 / sig ** 2))
+            kernel[i, :] /= np.sum(kernel[i, :])
+        out = np.empty((3, 2 * R + 1), dtype=np.float32)
+        out[0, :], out[1, :], out[2, :] = kernel[2, :], kernel[0, :], kernel[1, :]
+        return out
+
+    if psf is None:
+        k = _config([], False)
+        k[0, 0] = -1
+        return k
+    if isinstance(psf, str):
+        if psf == 'measured':
+            raise NotImplementedError("the measured mMR PSF comes from nimpa, which is not "
+                                      "available; pass FWHMs or a [3, 17] kernel")
+        raise ValueError(f'unrecognised PSF definition ({psf})')
+    if isinstance(psf, Real):
+        return _config([psf] * 3)
+    a = np.asanyarray(psf)
+    if a.shape == (3, 2 * R + 1):
+        k = _config([], False)
+        k[0, :], k[1, :], k[2, :] = a[2, :], a[0, :], a[1, :]
+        return k
+    if a.ndim == 1 and len(a) == 3:
+        return _config(list(a))
+    raise ValueError(f'invalid PSF dimensions ({a.shape})')
+
+
 def subset_table(params: dict, nsub: int = 14) -> np.ndarray:
     """`[nsub, 1 + Nprj]` int32 with column 0 = Nprj, as `sinoTIdx` in `osemone`."""
     rows = [get_subsets14(n, params)[0] for n in range(nsub)]

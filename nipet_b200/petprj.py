@@ -8,6 +8,8 @@ Errors raise Python exceptions instead of exiting the process.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -135,13 +137,19 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     (`prj_module.cu:613-839`, `recon.cu:318-521`).
 
     `subs` is `[Nsub, 1+Nprj]` with `subs[i,0] = Nprj`; `sensimg` is `[Nsub,320,320,127]`;
-    `krnl[0,0] < 0` means no resolution modelling (the only mode provided)."""
+    `krnl` `[3, 17]` is the resolution-modelling kernel (rows z, x, y as `psf_config`
+    builds them), `krnl[0,0] < 0` switching it off.  With a kernel the sensitivity images
+    are convolved on every call and the iteration convolves the image before each forward
+    projection and the back projection before the update, as the reference does
+    (`recon.cu:437-497`)."""
     dev = device_of(cnst)
     if int(cnst['SPN']) != 11:
         raise NotImplementedError('nipet_b200.petprj.osem runs span-11 data')
-    k = np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor) else krnl).reshape(-1)
-    if k.size and k[0] >= 0:
-        raise NotImplementedError('resolution modelling (PSF kernel) is not provided')
+    k = np.ascontiguousarray(np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor) else krnl,
+                                        dtype=np.float32).reshape(-1))
+    use_psf = k.size > 0 and k[0] >= 0
+    if use_psf and k.size != 3 * 17:
+        raise ValueError('krnl must have shape (3, 17)')
     g = get_geometry(txLUT, axLUT, dev)
     nsn = 837
     lib = _lib.load()
@@ -168,12 +176,25 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     m = to_device(msk, np.float32, dev)
     msk128 = (to_col128(m) > 0.5).to(torch.uint8)
     bimg128 = torch.empty_like(img128)
+    kp = k.ctypes.data_as(C.c_void_p)
+    if use_psf:
+        work = torch.empty((2, COL128), device=dev, dtype=torch.float32)
+        for i in range(nsub):  # the sensitivity images, convolved once per call
+            _lib.check(lib.nb_psf_col128(dev_ptr(sens128[i]), dev_ptr(sens128[i]), kp,
+                                         dev_ptr(work[0]), st))
     for i in range(nsub):
         nprj = int(subs_np[i, 0])
         d_sub = to_device(subs_np[i, 1:1 + nprj].astype(np.int32), np.int32, dev)
-        _lib.check(lib.nb_osem_subset(g.handle, dev_ptr(img128), dev_ptr(bimg128),
-                                      dev_ptr(sens128[i]), dev_ptr(msk128), dev_ptr(d_psng),
-                                      dev_ptr(rs), dev_ptr(d_sub), nprj, st))
+        if use_psf:
+            _lib.check(lib.nb_osem_subset_psf(g.handle, dev_ptr(img128), dev_ptr(bimg128),
+                                              dev_ptr(sens128[i]), dev_ptr(msk128),
+                                              dev_ptr(d_psng), dev_ptr(rs), dev_ptr(d_sub),
+                                              nprj, kp, dev_ptr(work), st))
+        else:
+            _lib.check(lib.nb_osem_subset(g.handle, dev_ptr(img128), dev_ptr(bimg128),
+                                          dev_ptr(sens128[i]), dev_ptr(msk128),
+                                          dev_ptr(d_psng), dev_ptr(rs), dev_ptr(d_sub), nprj,
+                                          st))
     out = from_col128(img128)
     g.check()
     _writeback(img, out[0])

@@ -34,12 +34,13 @@ def load():
         P, I = C.c_void_p, C.c_int
         lib.ref_fprj.argtypes = [P, P, P, I, I, I, P, P, P, P, P, P, I, P]
         lib.ref_bprj.argtypes = [P, P, P, I, I, P, P, P, P, P, I, P]
-        lib.ref_osem.argtypes = [P, P, P, P, P, P, P, P, I, I, P, P, P, P, P, P, I, I, P]
+        lib.ref_osem.argtypes = [P, P, P, P, P, P, P, P, I, I, P, P, P, P, P, P, I, I, P, P]
         lib.ref_tables.argtypes = [P, P, P, P, I]
         lib.ref_lminfo.argtypes = [C.c_char_p, I, P]
+        lib.ref_psf.argtypes = [P, P, P]
         lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
-                  lib.ref_hist):
+                  lib.ref_hist, lib.ref_psf):
             f.restype = I
         _lib = lib
     return _lib
@@ -95,23 +96,28 @@ def bprj(params, sino, subs=None, span=11):
     return out, ms.value
 
 
-def osem(params, img, msk, psng, rsng, ssng, nsng, asng, subs_table, sens, span=11):
-    """One reference OSEM iteration (all subsets), updating `img` in place; returns the
-    time of the call in ms (including the reference's own host<->device copies)."""
+def osem(params, img, msk, psng, rsng, ssng, nsng, asng, subs_table, sens, span=11, psf=None):
+    """One reference OSEM iteration (all subsets), updating `img` in place; psf: the
+    [3][17] resolution kernel or None.  Returns the time of the call in ms (including the
+    reference's own host<->device copies)."""
     L = _Luts(params, span)
     assert img.dtype == np.float32 and img.flags.c_contiguous and img.shape == IMG
-    msk = np.ascontiguousarray(msk, np.uint8)
-    psng = np.ascontiguousarray(psng, np.uint16)
     f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
-    tab = np.ascontiguousarray(subs_table, np.int32)
-    sens = f32(sens)
-    if sens.shape != (tab.shape[0],) + IMG:
+    # every converted array is held here until the call returns
+    arrs = {'msk': np.ascontiguousarray(msk, np.uint8),
+            'psng': np.ascontiguousarray(psng, np.uint16),
+            'rsng': f32(rsng), 'ssng': f32(ssng), 'nsng': f32(nsng), 'asng': f32(asng),
+            'tab': np.ascontiguousarray(subs_table, np.int32), 'sens': f32(sens),
+            'psf': None if psf is None else f32(psf)}
+    tab = arrs['tab']
+    if arrs['sens'].shape != (tab.shape[0],) + IMG:
         raise ValueError('one sensitivity image per subset is required')
     ms = C.c_float()
-    _check(load().ref_osem(_p(img), _p(msk), _p(psng), _p(f32(rsng)), _p(f32(ssng)),
-                           _p(f32(nsng)), _p(f32(asng)), _p(tab), tab.shape[0], tab.shape[1],
-                           _p(sens), _p(L.li2rng), _p(L.li2sn), _p(L.li2nos), _p(L.s2c),
-                           _p(L.crs), L.ncrs, span, C.byref(ms)), 'osem')
+    _check(load().ref_osem(_p(img), _p(arrs['msk']), _p(arrs['psng']), _p(arrs['rsng']),
+                           _p(arrs['ssng']), _p(arrs['nsng']), _p(arrs['asng']), _p(tab),
+                           tab.shape[0], tab.shape[1], _p(arrs['sens']), _p(L.li2rng),
+                           _p(L.li2sn), _p(L.li2nos), _p(L.s2c), _p(L.crs), L.ncrs, span,
+                           _p(arrs['psf']), C.byref(ms)), 'osem')
     return ms.value
 
 
@@ -152,3 +158,12 @@ def hist(params, path, span=11, t0=0, t1=0, btp=0, btprt=1.0):
                         C.byref(psm), C.byref(dsm), C.byref(ms)), 'hist')
     out['psum'], out['dsum'], out['nitag'], out['frame_s'] = psm.value, dsm.value, n, tt
     return out, ms.value
+
+
+def psf(img, krnl):
+    """The reference's PSF convolution (recon.cu d_pad + d_conv + d_unpad) of one image."""
+    x = np.ascontiguousarray(img, np.float32).reshape(IMG)
+    k = np.ascontiguousarray(krnl, np.float32).reshape(3, 17)
+    out = np.empty(IMG, np.float32)
+    _check(load().ref_psf(_p(out), _p(x), _p(k)), 'psf')
+    return out

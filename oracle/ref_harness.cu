@@ -21,6 +21,12 @@
 #include "prjf.h"
 #include "recon.h"
 
+// resolution-modelling routines of prj/src/recon.cu (defined there, not in its header)
+void setConvolutionKernel(float *krnl);
+void d_pad(float *dst, float *src, const int z);
+void d_unpad(float *dst, float *src, const int z);
+void d_conv(float *d_buff, float *d_imgout, float *d_imgint, int Nvk, int Nvj, int Nvi);
+
 namespace {
 
 Cnst make_cnst(int span) {
@@ -153,7 +159,8 @@ int ref_bprj(float *im, const float *sino, const int *subs, int nprj, int span,
 }
 
 // One OSEM iteration over all subsets by the reference's osem(), updating `img`
-// ([320][320][127], host) in place, as petprj.osem does with PSF off.  subs is the
+// ([320][320][127], host) in place, as petprj.osem does; psf: the [3][17] resolution
+// kernel, or NULL for none.  subs is the
 // [nsub][nprj1] table (column 0 = projections in the subset, then the LOR indices), sens
 // the [nsub][320][320][127] sensitivity images, msk a [320][320][127] byte mask (0/1),
 // psng [68516][nsinos] uint16, rsng/ssng/nsng/asng [68516][nsinos] float.  *ms: time of
@@ -162,9 +169,9 @@ int ref_osem(float *img, const uint8_t *msk, const uint16_t *psng, const float *
              const float *ssng, const float *nsng, const float *asng, const int *subs, int nsub,
              int nprj1, const float *sens, const float *li2rng, const int16_t *li2sn,
              const int8_t *li2nos, const int16_t *s2c, const float *crs, int ncrs, int span,
-             float *ms) {
+             const float *psf, float *ms) {
   float krnl[3 * KERNEL_LENGTH];
-  for (int i = 0; i < 3 * KERNEL_LENGTH; i++) krnl[i] = -1.f;
+  for (int i = 0; i < 3 * KERNEL_LENGTH; i++) krnl[i] = psf ? psf[i] : -1.f;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -276,6 +283,32 @@ int ref_hist(const char *fname, int tstart, int tstop, int span, int btp, float 
   if (psm) *psm = sp;
   if (dsm) *dsm = sd;
   return (int)err;
+}
+
+// The reference's PSF convolution of one image (recon.cu: d_pad, d_conv, d_unpad with the
+// kernel krnl [3][17]), host [320][320][127] in and out.
+int ref_psf(float *out, const float *in, const float *krnl) {
+  const size_t n = (size_t)SZ_IMX * SZ_IMY * SZ_IMZ, np = (size_t)SZ_IMX * SZ_IMY * (SZ_IMZ + 1);
+  float *d_in = nullptr, *d_src = nullptr, *d_dst = nullptr, *d_tmp = nullptr;
+  cudaError_t e = cudaMalloc(&d_in, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_src, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_dst, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_tmp, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(d_in, in, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    setConvolutionKernel(const_cast<float *>(krnl));
+    d_pad(d_src, d_in, 1);
+    d_conv(d_tmp, d_dst, d_src, SZ_IMX, SZ_IMY, SZ_IMZ + 1);
+    d_unpad(d_in, d_dst, 1);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d_in, n * sizeof(float), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d_in);
+  cudaFree(d_src);
+  cudaFree(d_dst);
+  cudaFree(d_tmp);
+  return (int)e;
 }
 
 }  // extern "C"

@@ -48,3 +48,25 @@ def test_dynamic_frame_counts_span_the_range():
     assert np.array_equal(c, c2)
     c3, _, _ = dynamic.frame_counts(16, seed=1)
     assert not np.array_equal(c, c3)
+
+
+def test_psf_config_mirrors_the_reference_rules():
+    from nipet_b200 import geometry, mmrrec
+    Cnt = geometry.get_mmrparams()['Cnt']
+    off = mmrrec.psf_config(None, Cnt)
+    assert off.shape == (3, 17) and off[0, 0] == -1
+    k = mmrrec.psf_config([3.0, 5.0, 4.0], Cnt)
+    assert np.allclose(k.sum(axis=1), 1.0)
+    # rows are z, x, y: the z row is the 4 mm kernel at 2.03 mm voxels
+    sig = mmrrec.fwhm2sig(4.0, voxsize=Cnt['SZ_VOXZ'] * 10)
+    x = np.arange(-8, 9)
+    g = np.exp(-0.5 * x ** 2 / sig ** 2)
+    assert np.allclose(k[0], g / g.sum(), rtol=1e-6)
+    assert k[1, 8] > k[2, 8]  # x (3 mm) is narrower than y (5 mm)
+    direct = np.arange(51, dtype=np.float32).reshape(3, 17)
+    kd = mmrrec.psf_config(direct, Cnt)
+    assert np.array_equal(kd[0], direct[2]) and np.array_equal(kd[1], direct[0])
+    with pytest.raises(NotImplementedError):
+        mmrrec.psf_config('measured', Cnt)
+    with pytest.raises(ValueError):
+        mmrrec.psf_config([1.0, 2.0], Cnt)
