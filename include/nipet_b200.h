@@ -176,6 +176,22 @@ int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens1
                          const float *rscale, int nrep, int bs, int tile, int span,
                          const int32_t *subs, int nprj, void *stream);
 
+/* ---- randoms from the delayed fan sums (lm/src/rnd.cu:169-386 gpu_randoms, driven by
+ * mmrhist.randoms / rand, lm/mmrhist.py:188-221) ---------------------------------------
+ * nb_randoms replaces gpu_randoms: crystal singles fitted to the delayed fan sums (ten
+ * damped fixed-point steps) and the randoms sinogram they imply.
+ *   rsn      dev [nsinos][252][344] float (Siemens layout with gaps, gaps 0), overwritten
+ *   cmap     dev [504][64] float singles per crystal (with gaps) and ring, overwritten
+ *   fansums  [64][504] uint32 (mmr_lmproc.hist's `fan`), host or device memory
+ *   crsr [504], cij [448][448], s2cr [68516][2], aw2sn [68516][2], sn1_rno [4084][2],
+ *   sn1_sn11 [4084] (txLUT crsri/cij/s2cr/aw2sn, axLUT sn1_rno/sn1_sn11), host int16/int8
+ *   span 1 or 11; mrd the maximum ring difference (60).
+ * Waits on `stream` for the fan sums, then runs asynchronously. */
+int nb_randoms(float *rsn, float *cmap, const uint32_t *fansums, const int16_t *crsr,
+               const int8_t *cij, const int16_t *s2cr, const int16_t *aw2sn,
+               const int16_t *sn1_rno, const int16_t *sn1_sn11, int span, int mrd,
+               void *stream);
+
 /* ---- list-mode histogramming (lm/src/lmproc.cu:12-230, hst.cu:37-528, lmaux.cu:17-270) -
  * nb_lm_plan replaces getLMinfo + modifyLMinfo: the chunk plan of a list-mode stream
  * (host [ele] int32 words), chunks cut at time tags with t % 100 ms == 0, and the time

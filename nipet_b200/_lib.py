@@ -54,6 +54,7 @@ SIGNATURES = {
     'nb_osem_rs': ([P, P, P, P, P, C.c_size_t, P], I),
     'nb_osem_subset': ([P, P, P, P, P, P, P, P, I, P], I),
     'nb_psf_col128': ([P, P, P, P, P], I),
+    'nb_randoms': ([P, P, P, P, P, P, P, P, P, I, I, P], I),
     'nb_osem_subset_psf': ([P, P, P, P, P, P, P, P, I, P, P, P], I),
     'nb_lm_plan': ([P, C.c_int64, I, I, I, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I),
                     C.POINTER(I), C.POINTER(I)], I),

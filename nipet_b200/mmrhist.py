@@ -75,3 +75,55 @@ def hist(datain, txLUT, axLUT, Cnt, t0=0, t1=0, cmass_sig=5, frms=None, use_stor
             'fansums': hstout['fan'], 'sngl_rate': single_rate, 'tsngl': t,
             'buckets': buckets, 'psino': hstout['psn'].astype(np.uint16),
             'dsino': hstout['dsn'].astype(np.uint16), 'pssr': hstout['ssr']}
+
+
+# ---------------------------------------------------------------------------------------
+# randoms from the delayed fan sums (lm/mmrhist.py:188-221, lm/src/rnd.cu:169-386)
+# ---------------------------------------------------------------------------------------
+def rand(fansums, txLUT, axLUT, Cnt):
+    """Randoms sinogram and crystal singles map from the delayed fan sums, as NIPET's
+    `mmrhist.rand` (`lm/mmrhist.py:207-221`): returns (rsn [nsinos, 252, 344] float32 in the
+    Siemens layout with gaps, cmap [504, 64] float32).  `fansums` is [64, 504] (numpy or a
+    CUDA tensor); span 1 or 11 from `Cnt['SPN']`."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib
+    from .device import dev_ptr, device_of, stream_ptr, to_device
+    span = int(Cnt['SPN'])
+    if span not in (1, 11):
+        raise NotImplementedError('randoms are provided for span 1 and 11')
+    nsn = Cnt['NSN11'] if span == 11 else Cnt['NSN1']
+    dev = device_of(Cnt)
+    d_f = to_device(np.asarray(fansums.cpu() if isinstance(fansums, torch.Tensor) else fansums)
+                    .reshape(-1).astype(np.uint32), np.uint32, dev)
+    if d_f.numel() != 64 * 504:
+        raise ValueError('fansums must hold 64 x 504 values')
+    luts = {'crsr': np.ascontiguousarray(txLUT['crsri'], np.int16),
+            'cij': np.ascontiguousarray(txLUT['cij'], np.int8),
+            's2cr': np.ascontiguousarray(txLUT['s2cr'], np.int16),
+            'aw2sn': np.ascontiguousarray(txLUT['aw2sn'], np.int16),
+            'sn1_rno': np.ascontiguousarray(axLUT['sn1_rno'], np.int16),
+            'sn1_sn11': np.ascontiguousarray(axLUT['sn1_sn11'], np.int16)}
+    rsn = torch.empty((nsn, 252, 344), device=dev)
+    cmap = torch.empty((504, 64), device=dev)
+    hp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    _lib.check(_lib.load().nb_randoms(dev_ptr(rsn), dev_ptr(cmap), dev_ptr(d_f),
+                                      *[hp(luts[k]) for k in ('crsr', 'cij', 's2cr', 'aw2sn',
+                                                              'sn1_rno', 'sn1_sn11')],
+                                      span, int(Cnt.get('MRD', 60)), stream_ptr(dev)))
+    return rsn.cpu().numpy(), cmap.cpu().numpy()
+
+
+def randoms(hst, scanner_params, gpu_dim=False):
+    """Estimated randoms sinogram from the delayeds' fan sums in a histogram dictionary
+    (`hst['fansums']`), as NIPET's `mmrhist.randoms` (`lm/mmrhist.py:188-204`): returns
+    (rsn, cmap), rsn in the gap-free [68516, nsinos] layout when `gpu_dim`."""
+    Cnt, txLUT, axLUT = (scanner_params['Cnt'], scanner_params['txLUT'],
+                         scanner_params['axLUT'])
+    rsn, cmap = rand(hst['fansums'], txLUT, axLUT, Cnt)
+    if gpu_dim:
+        from . import mmraux
+        return mmraux.remgaps(rsn, txLUT, Cnt), cmap
+    return rsn, cmap

@@ -1,5 +1,5 @@
 #!/bin/sh
-# Compile the reference's own CUDA projectors, OSEM and list-mode histogrammer (sources read in place from the
+# Compile the reference's own CUDA projectors, OSEM, list-mode histogrammer and randoms (sources read in place from the
 # reference tree, nothing copied) with the test-only harness oracle/ref_harness.cu into
 # oracle/_ref/libnipet_ref.so.  Flags follow the reference's Release build (-O3, no fast
 # math), for sm_100a.  Usage: oracle/build_ref.sh [reference root]
@@ -13,6 +13,6 @@ mkdir -p "$HERE/_ref"
   -DNIPET_CU_THREADS=1024 -I"$REF/include" -I"$REF/prj/src" -I"$REF/lm/src" \
   "$REF/prj/src/prjf.cu" "$REF/prj/src/prjb.cu" "$REF/prj/src/tprj.cu" \
   "$REF/prj/src/recon.cu" "$REF/lm/src/lmproc.cu" "$REF/lm/src/hst.cu" \
-  "$REF/lm/src/lmaux.cu" "$REF/src/scanner_0.cu" "$HERE/ref_harness.cu" \
+  "$REF/lm/src/lmaux.cu" "$REF/lm/src/rnd.cu" "$REF/src/scanner_0.cu" "$HERE/ref_harness.cu" \
   -lcurand -o "$HERE/_ref/libnipet_ref.so"
 echo "$HERE/_ref/libnipet_ref.so"

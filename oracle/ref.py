@@ -38,9 +38,10 @@ def load():
         lib.ref_tables.argtypes = [P, P, P, P, I]
         lib.ref_lminfo.argtypes = [C.c_char_p, I, P]
         lib.ref_psf.argtypes = [P, P, P]
+        lib.ref_randoms.argtypes = [P] * 9 + [I]
         lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
-                  lib.ref_hist, lib.ref_psf):
+                  lib.ref_hist, lib.ref_psf, lib.ref_randoms):
             f.restype = I
         _lib = lib
     return _lib
@@ -167,3 +168,22 @@ def psf(img, krnl):
     out = np.empty(IMG, np.float32)
     _check(load().ref_psf(_p(out), _p(x), _p(k)), 'psf')
     return out
+
+
+def randoms(params, fansums, span=11):
+    """The reference's gpu_randoms on [64, 504] fan sums: (rsn [nsinos, 252, 344], cmap
+    [504, 64]) float32."""
+    tx, ax = params['txLUT'], params['axLUT']
+    a = {'fan': np.ascontiguousarray(fansums, np.uint32).reshape(64, 504),
+         'crsr': np.ascontiguousarray(tx['crsri'], np.int16),
+         'cij': np.ascontiguousarray(tx['cij'], np.int8),
+         's2cr': np.ascontiguousarray(tx['s2cr'], np.int16),
+         'aw2sn': np.ascontiguousarray(tx['aw2sn'], np.int16),
+         'rno': np.ascontiguousarray(ax['sn1_rno'], np.int16),
+         's11': np.ascontiguousarray(ax['sn1_sn11'], np.int16)}
+    rsn = np.zeros((837 if span == 11 else 4084, 252, 344), np.float32)
+    cmap = np.zeros((504, 64), np.float32)
+    _check(load().ref_randoms(_p(rsn), _p(cmap), _p(a['fan']), _p(a['crsr']), _p(a['cij']),
+                              _p(a['s2cr']), _p(a['aw2sn']), _p(a['rno']), _p(a['s11']), span),
+           'randoms')
+    return rsn, cmap

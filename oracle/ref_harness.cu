@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include "lmproc.h"
+#include "rnd.h"
 #include "prjb.h"
 #include "prjf.h"
 #include "recon.h"
@@ -308,6 +309,33 @@ int ref_psf(float *out, const float *in, const float *krnl) {
   cudaFree(d_src);
   cudaFree(d_dst);
   cudaFree(d_tmp);
+  return (int)e;
+}
+
+// Randoms from the delayed fan sums by the reference's gpu_randoms (lm/src/rnd.cu:169-386),
+// as mmr_lmproc.rand calls it (lm_module.cu:396-560): host arrays in and out -- rsn
+// [nsinos][252][344], cmap [504][64], fansums [64][504]; txLUT crsri/cij/s2cr/aw2sn and
+// axLUT sn1_rno/sn1_sn11.
+int ref_randoms(float *rsn, float *cmap, const uint32_t *fansums, const int16_t *crsr,
+                const int8_t *cij, const int16_t *s2cr, const int16_t *aw2sn,
+                const int16_t *sn1_rno, const int16_t *sn1_sn11, int span) {
+  Cnst c = make_cnst(span);
+  c.A = NSANGLES;
+  c.W = NSBINS;
+  c.NCRS = nCRS;
+  c.NCRSR = nCRSR;
+  c.MRD = mxRD;
+  txLUTs tx;
+  std::memset(&tx, 0, sizeof(tx));
+  tx.s2cr = reinterpret_cast<LORcc *>(const_cast<int16_t *>(s2cr));
+  tx.aw2sn = reinterpret_cast<LORaw *>(const_cast<int16_t *>(aw2sn));
+  tx.cij = reinterpret_cast<char *>(const_cast<int8_t *>(cij));
+  tx.crsr = const_cast<short *>(crsr);
+  tx.naw = AW;
+  gpu_randoms(rsn, cmap, const_cast<unsigned int *>(fansums), tx,
+              const_cast<short *>(sn1_rno), const_cast<short *>(sn1_sn11), c);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
   return (int)e;
 }
 

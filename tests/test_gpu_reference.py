@@ -131,3 +131,27 @@ def test_histogram_bit_exact_with_reference(params, cuda_device, tmp_path, nev, 
         b = o[k].cpu().numpy().reshape(-1)[:a.size].astype(a.dtype)
         assert np.array_equal(a, b), f'{k}: {int(np.sum(a != b))} bins differ'
     np.testing.assert_array_equal(r['mss'], o['mss'].cpu().numpy().reshape(-1)[:r['mss'].size])
+
+
+@pytest.mark.parametrize('span', [11, 1])
+def test_randoms_match_reference(params, cuda_device, span):
+    """Randoms from the delayed fan sums of a synthetic stream: the singles map and the
+    randoms sinogram against the reference's gpu_randoms, relative 1e-5 (float sums in a
+    different order)."""
+    from nipet_b200 import mmr_lmproc, mmrhist, phantoms
+    lm = phantoms.lm_stream_fast(8_000_000, 20, params=params, seed=6, device=cuda_device)
+    o = mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'],
+                               dict(params['Cnt'], SPN=11, BTP=0))
+    fan = o['fan'].cpu().numpy()
+    assert fan.sum() > 0
+    rr, rc = ref.randoms(params, fan, span=span)
+    Cnt = dict(params['Cnt'], SPN=span)
+    gr, gc = mmrhist.rand(fan, params['txLUT'], params['axLUT'], Cnt)
+    active = params['txLUT']['crsri'] >= 0
+    assert np.all(gc[~active] == 0) and np.all(rc[~active] == 0)
+    relc = np.abs(gc - rc)[active] / np.abs(rc[active])
+    assert relc.max() <= 1e-5, f'singles map: {relc.max():.3e}'
+    big = rr >= 1e-3 * rr.max()
+    rel = np.abs(gr - rr)[big] / rr[big]
+    assert rel.max() <= 1e-5, f'randoms sinogram: {rel.max():.3e}'
+    assert np.all(gr[~big] <= 1e-3 * rr.max() * (1 + 1e-5))
