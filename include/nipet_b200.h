@@ -176,6 +176,22 @@ int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const float *sens1
                          const float *rscale, int nrep, int bs, int tile, int span,
                          const int32_t *subs, int nprj, void *stream);
 
+/* ---- normalisation sinogram (src/norm.cu:13-210 norm_from_components, driven by
+ * mmrnorm.get_norm_sino, mmrnorm.py:155-195) --------------------------------------------
+ * nb_norm replaces norm_from_components: the norm sinogram from the Siemens components
+ * (read from the norm file by the caller) and the average bucket singles.
+ *   sng  dev [68516][nsinos] float (gap-free), overwritten
+ *   geo [>=344] (first segment row of the geometric effects), cinf [344][9] crystal
+ *   interference, ceff [64][504] crystal efficiencies, axe1 [837] axial effects, axf1
+ *   [4084] span-1 axial factors (span 1 only, else may be NULL), dtp/dtnp [64]
+ *   dead-time parameters, buckets [224] int32 average singles (mmrhist's `buckets`),
+ *   sn1_rno [4084][2], sn1_sn11 [4084], sn1_sn11no [4084], aw2ali [68516]; all host.
+ *   span 1 or 11. */
+int nb_norm(float *sng, const float *geo, int ngeo, const float *cinf, const float *ceff,
+            const float *axe1, const float *axf1, const float *dtp, const float *dtnp,
+            const int32_t *buckets, const int16_t *sn1_rno, const int16_t *sn1_sn11,
+            const int8_t *sn1_sn11no, const int32_t *aw2ali, int span, void *stream);
+
 /* ---- randoms from the delayed fan sums (lm/src/rnd.cu:169-386 gpu_randoms, driven by
  * mmrhist.randoms / rand, lm/mmrhist.py:188-221) ---------------------------------------
  * nb_randoms replaces gpu_randoms: crystal singles fitted to the delayed fan sums (ten

@@ -55,6 +55,7 @@ SIGNATURES = {
     'nb_osem_subset': ([P, P, P, P, P, P, P, P, I, P], I),
     'nb_psf_col128': ([P, P, P, P, P], I),
     'nb_randoms': ([P, P, P, P, P, P, P, P, P, I, I, P], I),
+    'nb_norm': ([P, P, I, P, P, P, P, P, P, P, P, P, P, P, I, P], I),
     'nb_osem_subset_psf': ([P, P, P, P, P, P, P, P, I, P, P, P], I),
     'nb_lm_plan': ([P, C.c_int64, I, I, I, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I),
                     C.POINTER(I), C.POINTER(I)], I),

@@ -216,3 +216,45 @@ def hist(lm, params, t0=0, t1=0, span=11, btp=0, btprt=1.0, seed=0, rep=0) -> di
             'ssr': ssrb.reshape(127, 252, 344), 'phc': phc, 'dhc': dhc, 'mss': mss,
             'pvs': pvs.reshape(-1, 127, 344), 'fan': fan.reshape(64, 504),
             'bck': bck.reshape(2, nitag, 224), 'plan': plan}
+
+
+def norm_sino(normcomp: dict, buckets, params: dict, span: int = 11, lors=None) -> np.ndarray:
+    """Float64 normalisation factors [len(lors), nsinos] for the gap-free LORs `lors` (all
+    68516 by default), restating the reference's dev_norm (src/norm.cu:13-48): crystal pair
+    of each LOR from its full linear index, geometric x interference x both crystal
+    efficiencies x both dead-time factors exp(x dtp / (1 + x dtnp)) / (1 + x dtnp) with x
+    half the crystal's bucket singles (28 x 8 buckets of 18 x 8 crystals); span 1 scaled by
+    axf1 / axe1 of its span-11 sinogram, span 11 the sum of factor / (axe1 * planes) over the
+    sinogram's span-1 planes."""
+    tx, ax = params['txLUT'], params['axLUT']
+    ali = np.asarray(tx['aw2ali'], np.int64)
+    if lors is not None:
+        ali = ali[np.asarray(lors)]
+    W, NCRS = 344, 504
+    wi = ali % W
+    ai = (ali - wi) // W
+    c1 = np.floor(np.fmod(ai + 0.5 * (NCRS - 2 + W // 2 - wi), NCRS)).astype(np.int64)
+    c2 = np.floor(np.fmod(ai + 0.5 * (2 * NCRS - 2 - W // 2 + wi), NCRS)).astype(np.int64)
+    geo = np.asarray(normcomp['geo'], np.float64).reshape(-1)[:W]
+    cinf = np.asarray(normcomp['cinf'], np.float64).reshape(W, 9)
+    ceff = np.asarray(normcomp['ceff'], np.float64).reshape(64, NCRS)
+    axe1 = np.asarray(normcomp['axe1'], np.float64)
+    dtp = np.asarray(normcomp['dtp'], np.float64)
+    dtnp = np.asarray(normcomp['dtnp'], np.float64)
+    bck = np.asarray(buckets, np.float64).reshape(-1)
+    rno = np.asarray(ax['sn1_rno'], np.int64).reshape(-1, 2)
+    s11 = np.asarray(ax['sn1_sn11'], np.int64)
+    nos = np.asarray(ax['sn1_sn11no'], np.float64)
+    r = np.arange(64)[:, None]
+    b = np.arange(NCRS)[None, :] // 18 + 28 * (r // 8)
+    x = 0.5 * bck[b]
+    den = 1.0 + x * dtnp[:, None]
+    crys = ceff * np.exp(x * dtp[:, None] / den) / den     # [ring][crystal]
+    gc = geo[wi] * cinf[wi, ai % 9]
+    f = gc[:, None] * crys[rno[:, 0]][:, c1].T * crys[rno[:, 1]][:, c2].T  # [lor][plane]
+    if span == 1:
+        axf1 = np.asarray(normcomp['axf1'], np.float64)
+        return f * (axf1 / axe1[s11])[None, :]
+    out = np.zeros((len(ali), 837))
+    np.add.at(out.T, s11, (f / (axe1[s11] * nos)[None, :]).T)
+    return out

@@ -39,6 +39,7 @@ def load():
         lib.ref_lminfo.argtypes = [C.c_char_p, I, P]
         lib.ref_psf.argtypes = [P, P, P]
         lib.ref_randoms.argtypes = [P] * 9 + [I]
+        lib.ref_norm.argtypes = [P, P, I] + [P] * 11 + [I]
         lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
                   lib.ref_hist, lib.ref_psf, lib.ref_randoms):
@@ -187,3 +188,23 @@ def randoms(params, fansums, span=11):
                               _p(a['s2cr']), _p(a['aw2sn']), _p(a['rno']), _p(a['s11']), span),
            'randoms')
     return rsn, cmap
+
+
+def norm(params, normcomp, buckets, span=11):
+    """The reference's norm_from_components: gap-free [68516, nsinos] float32."""
+    tx, ax = params['txLUT'], params['axLUT']
+    f = lambda k: np.ascontiguousarray(normcomp[k], np.float32)  # noqa: E731
+    a = {'geo': f('geo'), 'cinf': f('cinf'), 'ceff': f('ceff'), 'axe1': f('axe1'),
+         'axf1': f('axf1') if 'axf1' in normcomp else np.ones(4084, np.float32),
+         'dtp': f('dtp'), 'dtnp': f('dtnp'),
+         'bck': np.ascontiguousarray(buckets, np.int32),
+         'rno': np.ascontiguousarray(ax['sn1_rno'], np.int16),
+         's11': np.ascontiguousarray(ax['sn1_sn11'], np.int16),
+         'nos': np.ascontiguousarray(ax['sn1_sn11no'], np.int8),
+         'aw': np.ascontiguousarray(tx['aw2ali'], np.int32)}
+    out = np.zeros((68516, 837 if span == 11 else 4084), np.float32)
+    _check(load().ref_norm(_p(out), _p(a['geo']), a['geo'].size // 344, _p(a['cinf']),
+                           _p(a['ceff']), _p(a['axe1']), _p(a['axf1']), _p(a['dtp']),
+                           _p(a['dtnp']), _p(a['bck']), _p(a['rno']), _p(a['s11']),
+                           _p(a['nos']), _p(a['aw']), span), 'norm')
+    return out

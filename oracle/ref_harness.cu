@@ -1,5 +1,5 @@
 // Test-only harness around the reference's own CUDA projectors, OSEM and list-mode
-// histogrammer.
+// histogrammer, randoms and normalisation.
 //
 // Built by oracle/build_ref.sh together with the reference sources
 // (niftypet/nipet/prj/src/{prjf,prjb,tprj,recon}.cu, lm/src/{lmproc,hst,lmaux}.cu and
@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include "lmproc.h"
+#include "norm.h"
 #include "rnd.h"
 #include "prjb.h"
 #include "prjf.h"
@@ -334,6 +335,45 @@ int ref_randoms(float *rsn, float *cmap, const uint32_t *fansums, const int16_t 
   tx.naw = AW;
   gpu_randoms(rsn, cmap, const_cast<unsigned int *>(fansums), tx,
               const_cast<short *>(sn1_rno), const_cast<short *>(sn1_sn11), c);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return (int)e;
+}
+
+// Normalisation sinogram from its components by the reference's norm_from_components
+// (src/norm.cu:54-210), as mmr_auxe.norm passes them (src/aux_module.cu:150-268): host
+// arrays in, gap-free sino [68516][nsinos] out.  geo [ngeo0][344], cinf [344][9], ceff
+// [64][504], axe1 [837], axf1 [4084] (read for both spans), dtp/dtnp [64], buckets [224];
+// axLUT sn1_rno/sn1_sn11/sn1_sn11no; txLUT aw2ali.
+int ref_norm(float *sino, const float *geo, int ngeo0, const float *cinf, const float *ceff,
+             const float *axe1, const float *axf1, const float *dtp, const float *dtnp,
+             const int *buckets, const int16_t *sn1_rno, const int16_t *sn1_sn11,
+             const int8_t *sn1_sn11no, const int *aw2ali, int span) {
+  Cnst c = make_cnst(span);
+  NormCmp n;
+  std::memset(&n, 0, sizeof(n));
+  n.geo = const_cast<float *>(geo);
+  n.cinf = const_cast<float *>(cinf);
+  n.ceff = const_cast<float *>(ceff);
+  n.axe1 = const_cast<float *>(axe1);
+  n.axf1 = const_cast<float *>(axf1);
+  n.dtp = const_cast<float *>(dtp);
+  n.dtnp = const_cast<float *>(dtnp);
+  n.ngeo[0] = ngeo0;
+  n.ngeo[1] = NSBINS;
+  n.ncinf[0] = NSBINS;
+  n.ncinf[1] = 9;
+  n.nceff[0] = NRINGS;
+  n.nceff[1] = nCRS;
+  n.naxe = NSINOS11;
+  n.nrdt = NRINGS;
+  axialLUT ax;
+  std::memset(&ax, 0, sizeof(ax));
+  ax.sn1_rno = const_cast<short *>(sn1_rno);
+  ax.sn1_sn11 = const_cast<short *>(sn1_sn11);
+  ax.sn1_sn11no = reinterpret_cast<char *>(const_cast<int8_t *>(sn1_sn11no));
+  ax.Nli2rno[1] = 2;
+  norm_from_components(sino, n, ax, const_cast<int *>(aw2ali), const_cast<int *>(buckets), c);
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   return (int)e;
