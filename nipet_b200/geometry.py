@@ -54,6 +54,8 @@ def get_mmr_constants() -> dict:
         'BPE': 4, 'LMOFF': 0, 'BTP': 0, 'BTPRT': 1.0, 'ITIME': 1000,
         # runtime
         'LOG': 30, 'DEVID': 0, 'SIGMA_RM': 0.0,
+        # decay / quantification corrections of osemone
+        'ISOTOPE': 'F18', 'DCYCRR': True,
     }
     return Cnt
 

@@ -85,6 +85,12 @@ def rand(fansums, txLUT, axLUT, Cnt):
     `mmrhist.rand` (`lm/mmrhist.py:207-221`): returns (rsn [nsinos, 252, 344] float32 in the
     Siemens layout with gaps, cmap [504, 64] float32).  `fansums` is [64, 504] (numpy or a
     CUDA tensor); span 1 or 11 from `Cnt['SPN']`."""
+    rsn, cmap = rand_dev(fansums, txLUT, axLUT, Cnt)
+    return rsn.cpu().numpy(), cmap.cpu().numpy()
+
+
+def rand_dev(fansums, txLUT, axLUT, Cnt):
+    """`rand` with both results left on the device (CUDA tensors)."""
     import ctypes as C
 
     import torch
@@ -96,8 +102,12 @@ def rand(fansums, txLUT, axLUT, Cnt):
         raise NotImplementedError('randoms are provided for span 1 and 11')
     nsn = Cnt['NSN11'] if span == 11 else Cnt['NSN1']
     dev = device_of(Cnt)
-    d_f = to_device(np.asarray(fansums.cpu() if isinstance(fansums, torch.Tensor) else fansums)
-                    .reshape(-1).astype(np.uint32), np.uint32, dev)
+    if isinstance(fansums, torch.Tensor):
+        d_f = fansums.to(dev).reshape(-1).contiguous()  # 32-bit counts
+        if d_f.element_size() != 4:
+            d_f = d_f.to(torch.int32)
+    else:
+        d_f = to_device(np.asarray(fansums).reshape(-1).astype(np.uint32), np.uint32, dev)
     if d_f.numel() != 64 * 504:
         raise ValueError('fansums must hold 64 x 504 values')
     luts = {'crsr': np.ascontiguousarray(txLUT['crsri'], np.int16),
@@ -113,7 +123,7 @@ def rand(fansums, txLUT, axLUT, Cnt):
                                       *[hp(luts[k]) for k in ('crsr', 'cij', 's2cr', 'aw2sn',
                                                               'sn1_rno', 'sn1_sn11')],
                                       span, int(Cnt.get('MRD', 60)), stream_ptr(dev)))
-    return rsn.cpu().numpy(), cmap.cpu().numpy()
+    return rsn, cmap
 
 
 def randoms(hst, scanner_params, gpu_dim=False):
@@ -127,3 +137,38 @@ def randoms(hst, scanner_params, gpu_dim=False):
         from . import mmraux
         return mmraux.remgaps(rsn, txLUT, Cnt), cmap
     return rsn, cmap
+
+
+def dynamic_timings(flist, offset=0):
+    """Start and end times of dynamic frames from their definition, as NIPET's function of
+    the same name (`lm/mmrhist.py:492-561`): `flist` is a 1-D list of frame durations
+    ([15, 15, 30, ...]) or ['def', [reps, duration], ...]; returns {'total', 'frames'
+    (uint16 durations), 'timings' (['timings', [t0, t1], ...])}."""
+    from collections.abc import Collection
+    from numbers import Integral
+    if not isinstance(flist, Collection) or isinstance(flist, str):
+        raise TypeError('Wrong type of frame data input')
+    if all(isinstance(t, Integral) for t in flist):
+        tsum = offset
+        t_frames = ['timings', [0, offset]] if offset > 0 else ['timings']
+        for d in flist:
+            t_frames.append([tsum, tsum + d])
+            tsum += d
+        return {'total': tsum, 'frames': np.uint16(flist), 'timings': t_frames}
+    if flist[0] == 'def' and all(isinstance(t, Collection) and len(t) == 2 for t in flist[1:]):
+        rows = [list(t) for t in flist[1:]]
+        if offset > 0:
+            # the reference prepends a definition of zero repetitions (no frame)
+            rows.insert(0, [0, offset])
+        farray = np.asarray(rows, dtype=np.uint16 if offset > 0 else None)
+        nfrm = int(np.sum(farray[:, 0]))
+        frms = np.zeros(nfrm, dtype=np.uint16)
+        tsum, fi, t_frames = 0, 0, ['timings']
+        for reps, dur in farray:
+            for _ in range(int(reps)):
+                t_frames.append([tsum, tsum + dur])
+                tsum += dur
+                frms[fi] = dur
+                fi += 1
+        return {'total': tsum, 'frames': frms, 'timings': t_frames}
+    raise TypeError('Unrecognised time frame definitions.')

@@ -6,23 +6,47 @@
   log-normal crystal efficiencies, uniform randoms, Poisson prompts), built on the GPU
   with this package's own projectors.
 * `Recon`: keeps LUTs, sinograms and the per-subset sensitivity images on the device and
-  runs OSEM iterations as fused sub-iteration kernels (`nb_osem_subset`) -- the OSEM
-  section of `osemone` (`prj/mmrrec.py:279-389`) without the per-call host transfers of
+  runs OSEM iterations as fused sub-iteration kernels (`nb_osem_subset`, or
+  `nb_osem_subset_psf` with a resolution-modelling kernel) -- the OSEM section of
+  `osemone` (`prj/mmrrec.py:279-389`) without the per-call host transfers of
   `petprj.osem` (`recon.cu:334-419`).
+* `osemone`: the reference's single-frame reconstruction (`prj/mmrrec.py:158-470`) on the
+  device: prompts, norm, attenuation, randoms and scatter sinograms are made or uploaded
+  once and stay resident for the sensitivity images and all iterations.
 """
 from __future__ import annotations
+
+import logging
+import os
+from collections import namedtuple
 
 import numpy as np
 import torch
 
 from . import _lib, geometry, phantoms
-from .device import dev_ptr, get_geometry, stream_ptr
+from .device import dev_ptr, device_of, get_geometry, stream_ptr
 from .geometry import get_subsets14
 from .petprj import COL128, from_col128, to_col128
 
-__all__ = ['get_subsets14', 'subset_table', 'synthetic_scan', 'Recon', 'norm_sinogram_gpu']
+__all__ = ['get_subsets14', 'subset_table', 'synthetic_scan', 'Recon', 'norm_sinogram_gpu',
+           'osemone', 'image_affine', 'RecOut', 'ISOTOPES']
+
+log = logging.getLogger(__name__)
 
 NAW = 68516
+
+# Half-life (s) and positron branching fraction of the isotopes NIPET's decay and
+# quantification corrections look up (its `resources.riLUT`, in the un-vendored `ninst`
+# package); published nuclear data.
+ISOTOPES = {
+    'F18': {'thalf': 109.77 * 60, 'BF': 0.967},
+    'C11': {'thalf': 20.38 * 60, 'BF': 0.998},
+    'O15': {'thalf': 122.24, 'BF': 0.999},
+    'Ga68': {'thalf': 67.71 * 60, 'BF': 0.891},
+    'Ge68': {'thalf': 270.95 * 24 * 3600, 'BF': 0.891},
+}
+
+RecOut = namedtuple('RecOut', 'im, fpet, imsmo, fsmo, affine')
 
 
 def fwhm2sig(fwhm, voxsize=1.0):
@@ -130,10 +154,13 @@ def synthetic_scan(params: dict, device, seed: int = 0, counts: float = 3e7,
 
 
 class Recon:
-    """Device-resident OSEM (span 11, PSF off) for one scan."""
+    """Device-resident OSEM (span 11) for one scan; `krnl` [3, 17] (as `psf_config` builds
+    it, `krnl[0, 0] < 0` = off) switches on resolution modelling: the sensitivity images
+    are convolved once and every sub-iteration convolves the image before the forward
+    projection and the back projection before the update (`recon.cu:437-497`)."""
 
     def __init__(self, params: dict, psng, rsng, nsng, asng, ssng=None, device=None,
-                 nsub: int = 14, mask_radius: float = 29.0):
+                 nsub: int = 14, mask_radius: float = 29.0, krnl=None):
         self.device = torch.device(device or 'cuda')
         self.params = params
         self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
@@ -160,6 +187,15 @@ class Recon:
         self.an = (self.asng * self.nsng).contiguous()
         self.sens128 = torch.empty((self.nsub, COL128), device=dev)
         self.bimg128 = torch.empty(COL128, device=dev)
+        self.krnl = None
+        if krnl is not None:
+            k = np.ascontiguousarray(np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor)
+                                                else krnl, np.float32).reshape(-1))
+            if k.size and k[0] >= 0:
+                if k.size != 3 * 17:
+                    raise ValueError('krnl must have shape (3, 17)')
+                self.krnl = k
+                self.work = torch.empty((2, COL128), device=dev)
         self.launches = 0
 
     def sensitivity(self):
@@ -170,6 +206,12 @@ class Recon:
                                                dev_ptr(self.an), dev_ptr(self.subs[i]),
                                                self.nprj, 11, st))
             self.launches += 1
+            if self.krnl is not None:
+                _lib.check(self.lib.nb_psf_col128(dev_ptr(self.sens128[i]),
+                                                  dev_ptr(self.sens128[i]),
+                                                  self.krnl.ctypes.data, dev_ptr(self.work[0]),
+                                                  st))
+                self.launches += 3
 
     def init_image(self) -> torch.Tensor:
         ones = torch.ones((320, 320, 127), device=self.device)
@@ -178,6 +220,14 @@ class Recon:
 
     def subiteration(self, img128: torch.Tensor, i: int, stream=None):
         st = stream if stream is not None else stream_ptr(self.device)
+        if self.krnl is not None:
+            _lib.check(self.lib.nb_osem_subset_psf(
+                self.geom.handle, dev_ptr(img128), dev_ptr(self.bimg128),
+                dev_ptr(self.sens128[i]), dev_ptr(self.msk128), dev_ptr(self.psng),
+                dev_ptr(self.rs), dev_ptr(self.subs[i]), self.nprj, self.krnl.ctypes.data,
+                dev_ptr(self.work), st))
+            self.launches += 8  # two 3-pass convolutions, the fused kernel, the update
+            return
         _lib.check(self.lib.nb_osem_subset(self.geom.handle, dev_ptr(img128),
                                            dev_ptr(self.bimg128), dev_ptr(self.sens128[i]),
                                            dev_ptr(self.msk128), dev_ptr(self.psng),
@@ -200,3 +250,144 @@ class Recon:
 
     def image(self, img128: torch.Tensor) -> torch.Tensor:
         return from_col128(img128.reshape(1, -1))[0]
+
+
+def image_affine(datain, Cnt: dict, gantry_offset: bool = False) -> np.ndarray:
+    """4x4 affine (mm) of the Siemens-layout image (`img/mmrimg.py:96-118`); the bed
+    position comes from `datain['hbed']` (cm, 0 if absent) instead of the DICOM header."""
+    if gantry_offset:
+        raise NotImplementedError('the gantry offset is read from the list-mode header, '
+                                  'which this package does not parse')
+    hbed = float((datain or {}).get('hbed', 0.0))
+    imz = Cnt['rSO_IMZ'] if ('rNRNG' in Cnt and 'rSO_IMZ' in Cnt) else Cnt['SO_IMZ']
+    B = np.diag(np.array([-10 * Cnt['SO_VXX'], 10 * Cnt['SO_VXY'], 10 * Cnt['SO_VXZ'], 1.]))
+    B[0, 3] = 10 * (.5 * Cnt['SO_IMX'] * Cnt['SO_VXX'])
+    B[1, 3] = 10 * ((-.5 * Cnt['SO_IMY'] + 1) * Cnt['SO_VXY'])
+    B[2, 3] = 10 * ((-.5 * imz + 1) * Cnt['SO_VXZ'] + hbed)
+    return B
+
+
+def _gapfree(x, txLUT, Cnt, dev, dtype):
+    """A sinogram as a gap-free [68516, nsinos] CUDA tensor of `dtype`, from the Siemens
+    [nsinos, 252, 344] layout or an already gap-free array / tensor."""
+    from . import mmraux
+    t = x if isinstance(x, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(x))
+    t = t.to(dev)
+    if t.dim() == 3:
+        t = mmraux.remgaps(t.to(dtype).contiguous(), txLUT, Cnt)
+    if t.dim() != 2 or t.shape[0] != NAW:
+        raise ValueError(f'sinogram of shape {tuple(x.shape)} is neither [nsinos, 252, 344] '
+                         f'nor [{NAW}, nsinos]')
+    return t.to(dtype).contiguous()
+
+
+def attenuation_sino(mus, params: dict, device) -> torch.Tensor:
+    """Attenuation factors exp(-integral of mu) [68516, 837] on the device for a GPU-layout
+    (320, 320, 127) mu-map in 1/cm (`petprj.fprj(..., att=1)` over all LORs)."""
+    geom = get_geometry(params['txLUT'], params['axLUT'], device)
+    mu = (mus if isinstance(mus, torch.Tensor) else torch.from_numpy(
+        np.ascontiguousarray(mus, np.float32))).to(device, torch.float32).contiguous()
+    asng = torch.empty((NAW, 837), device=device)
+    _lib.check(_lib.load().nb_fprj(geom.handle, dev_ptr(asng), dev_ptr(mu), None, NAW, 11, 1,
+                                   stream_ptr(device)))
+    return asng
+
+
+def decay_quant_factors(hst: dict, Cnt: dict, ncmp: dict, decay_ref_time=None):
+    """(dcycrr, qf, qf_loc) as `osemone` derives them (`prj/mmrrec.py:309-333`); a norm
+    without the DICOM header's quantification factor (`qf`) gives qf = qf_loc = 1."""
+    iso = ISOTOPES[Cnt.get('ISOTOPE', 'F18')]
+    lmbd = np.log(2) / iso['thalf']
+    if 't0' in hst and 'dur' in hst:
+        if Cnt.get('DCYCRR', True):
+            tref = decay_ref_time if decay_ref_time is not None else hst['t0']
+            dcycrr = np.exp(lmbd * tref) * lmbd * hst['dur'] / (1 - np.exp(-lmbd * hst['dur']))
+        else:
+            dcycrr = 1.
+        if ncmp.get('qf') is None:
+            log.warning('norm components carry no quantification factor: qf = 1')
+            return dcycrr, 1., 1.
+        return dcycrr, ncmp['qf'] / iso['BF'] / float(hst['dur']), ncmp.get('qf_loc', 1.)
+    return 1., 1., 1.
+
+
+def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=None,
+            mask_radius=29., decay_ref_time=None, attnsino=None, sctsino=None, randsino=None,
+            normcomp=None, emmskS=False, frmno='', fcomment='', outpath=None, fout=None,
+            store_img=False, store_itr=None, ret_sinos=False):
+    """OSEM reconstruction of one frame, as NIPET's `osemone` (`prj/mmrrec.py:158-470`),
+    with every sinogram on the device: prompts (`hst['psino']`), the norm from its
+    components and the frame's bucket singles, attenuation factors from the mu-maps
+    (`mumaps` = [hardware, object], Siemens layout, 1/cm) or `attnsino`, randoms from the
+    delayeds' fan sums or `randsino`, scatter from `sctsino`; then per-subset sensitivity
+    images and `itr` OSEM iterations (PSF from `psf_config(psf)`), the decay and
+    quantification factors, and the Siemens-layout image (Gaussian post-smoothing when
+    `fwhm` > 0).  Returns `RecOut(im, fpet, imsmo, fsmo, affine)`.
+
+    Modes: 0 (randoms only), 1 (+ attenuation), 2 (+ the given scatter).  Mode 3 (scatter
+    re-estimated between iterations by `sct/`) and NIfTI output (`store_img`,
+    `store_itr`) are not provided."""
+    from . import geometry as geo
+    from . import mmrhist, mmrnorm
+    from scipy import ndimage as ndi
+    Cnt, txLUT, axLUT = (scanner_params['Cnt'], scanner_params['txLUT'],
+                         scanner_params['axLUT'])
+    if int(Cnt['SPN']) != 11:
+        raise NotImplementedError('osemone reconstructs span-11 data (as petprj.osem)')
+    if recmod >= 3:
+        raise NotImplementedError('scatter estimation (sct/) is not provided: use recmod=2 '
+                                  'with sctsino, or recmod 0/1')
+    if recmod == 2 and sctsino is None:
+        raise ValueError('recmod 2 needs the scatter sinogram (sctsino)')
+    if store_img or store_itr:
+        raise NotImplementedError('NIfTI output is not provided: use the returned image')
+    dev = device_of(Cnt)
+    log.info('reconstruction in mode: %d', recmod)
+    psng = _gapfree(hst['psino'], txLUT, Cnt, dev, torch.uint16)
+    # norm
+    ncmp = normcomp if normcomp is not None else mmrnorm.get_components(datain, Cnt)
+    nsng = mmrnorm.norm_sino(ncmp, hst['buckets'], axLUT, txLUT, Cnt)
+    # attenuation factors
+    if recmod == 0:
+        asng = torch.ones((NAW, 837), device=dev)
+    elif attnsino is not None:
+        asng = _gapfree(attnsino, txLUT, Cnt, dev, torch.float32)
+    else:
+        muh, muo = mumaps
+        mus = geo.convert2dev(np.asarray(muo, np.float32) + np.asarray(muh, np.float32), Cnt)
+        asng = attenuation_sino(mus, scanner_params, dev)
+    # randoms
+    if randsino is not None:
+        rsng = _gapfree(randsino, txLUT, Cnt, dev, torch.float32)
+    else:
+        rsn, _ = mmrhist.rand_dev(hst['fansums'], txLUT, axLUT, Cnt)
+        rsng = _gapfree(rsn, txLUT, Cnt, dev, torch.float32)
+    ssng = _gapfree(sctsino, txLUT, Cnt, dev, torch.float32) if recmod == 2 else None
+    rec = Recon(scanner_params, psng, rsng, nsng, asng, ssng, device=dev,
+                mask_radius=mask_radius, krnl=psf_config(psf, Cnt))
+    rec.sensitivity()
+    img = rec.init_image()
+    for k in range(itr):
+        rec.iterate(img, 1)
+        if float(img.sum()) < 0.1:
+            log.warning('it seems there is not enough true data to render reasonable image')
+            itr = k
+            break
+    rec.geom.check()
+    dcycrr, qf, qf_loc = decay_quant_factors(hst, Cnt, ncmp, decay_ref_time)
+    x = rec.image(img).cpu().numpy() * np.float32(dcycrr * qf * qf_loc)
+    im = geo.convert2e7(x, Cnt)
+    opth = outpath if outpath is not None else os.path.join(datain.get('corepath', ''),
+                                                            'reconstructed')
+    if fout is None:
+        fpet = os.path.join(opth, os.path.basename(datain.get('lm_bf', 'lm')).split('.')[0] +
+                            f"{frmno}_t{hst.get('t0')}-{hst.get('t1')}sec_itr{itr}{fcomment}"
+                            '.nii.gz')
+    else:
+        fpet = os.path.join(opth, os.path.basename(fout).split('.')[0] +
+                            f'_itr{itr}{fcomment}.nii.gz')
+    im_smo = fsmo = None
+    if fwhm > 0:
+        im_smo = ndi.gaussian_filter(im, fwhm2sig(fwhm, voxsize=Cnt['SZ_VOXY'] * 10),
+                                     mode='mirror')
+    return RecOut(im, fpet, im_smo, fsmo, image_affine(datain, Cnt))

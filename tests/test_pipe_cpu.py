@@ -1,0 +1,82 @@
+"""Host logic of the reconstruction chain: frame definitions (`dynamic_timings`,
+`frame_timings`), the decay / quantification factors, the image affine, and the argument
+checks of `osemone` / `mmrchain` that stop before any device work.  No GPU calls."""
+import numpy as np
+import pytest
+
+from nipet_b200 import mmrhist, mmrrec, pipe
+
+
+def test_dynamic_timings_1d_and_def():
+    d = mmrhist.dynamic_timings([15, 15, 30])
+    assert d['timings'] == ['timings', [0, 15], [15, 30], [30, 60]] and d['total'] == 60
+    assert d['frames'].dtype == np.uint16 and list(d['frames']) == [15, 15, 30]
+    d = mmrhist.dynamic_timings([10, 20], offset=5)
+    assert d['timings'] == ['timings', [0, 5], [5, 15], [15, 35]] and d['total'] == 35
+    d = mmrhist.dynamic_timings(['def', [2, 15], [1, 60]])
+    assert d['timings'][1:] == [[0, 15], [15, 30], [30, 90]] and d['total'] == 90
+    assert list(d['frames']) == [15, 15, 60]
+    # offset in 'def' form: a zero-repetition definition, frames unchanged
+    d = mmrhist.dynamic_timings(['def', [2, 15]], offset=7)
+    assert d['timings'][1:] == [[0, 15], [15, 30]]
+    with pytest.raises(TypeError):
+        mmrhist.dynamic_timings('15,15')
+    with pytest.raises(TypeError):
+        mmrhist.dynamic_timings(['x', [1, 2]])
+
+
+def test_frame_timings_forms():
+    assert pipe.frame_timings(['fluid', [0, 0]]) == [[0, 0]]
+    assert pipe.frame_timings(['timings', [0, 10], [10, 25]]) == [[0, 10], [10, 25]]
+    assert pipe.frame_timings(['def', [3, 10]]) == [[0, 10], [10, 20], [20, 30]]
+    assert pipe.frame_timings([5, 5]) == [[0, 5], [5, 10]]
+    with pytest.raises(TypeError):
+        pipe.frame_timings((5, 5))
+    with pytest.raises(TypeError):
+        pipe.frame_timings(['fluid', [0, 1, 2]])
+
+
+def test_decay_and_quantification_factors(params):
+    Cnt = dict(params['Cnt'])
+    hst = {'t0': 100, 't1': 400, 'dur': 300}
+    lmbd = np.log(2) / (109.77 * 60)
+    d, q, ql = mmrrec.decay_quant_factors(hst, Cnt, {})
+    want = np.exp(lmbd * 100) * lmbd * 300 / (1 - np.exp(-lmbd * 300))
+    assert np.isclose(d, want, rtol=1e-12) and q == 1. and ql == 1.
+    d, q, ql = mmrrec.decay_quant_factors(hst, Cnt, {'qf': 2.5, 'qf_loc': 0.205},
+                                          decay_ref_time=0)
+    assert np.isclose(d, lmbd * 300 / (1 - np.exp(-lmbd * 300)))
+    assert np.isclose(q, 2.5 / 0.967 / 300) and ql == 0.205
+    d, q, ql = mmrrec.decay_quant_factors(hst, dict(Cnt, DCYCRR=False), {'qf': 1.0})
+    assert d == 1. and np.isclose(q, 1 / 0.967 / 300) and ql == 1.
+    assert mmrrec.decay_quant_factors({}, Cnt, {'qf': 3.0}) == (1., 1., 1.)
+
+
+def test_image_affine(params):
+    Cnt = params['Cnt']
+    B = mmrrec.image_affine({'hbed': 2.0}, Cnt)
+    assert B.shape == (4, 4)
+    assert np.isclose(B[0, 0], -2.08626) and np.isclose(B[2, 2], 2.03125)
+    assert np.isclose(B[0, 3], 10 * 0.5 * 344 * 0.208626)
+    assert np.isclose(B[2, 3], 10 * ((-63.5 + 1) * 0.203125 + 2.0))
+
+
+def test_osemone_and_mmrchain_argument_checks(params):
+    hst = {'psino': np.zeros((837, 252, 344), np.uint16)}
+    mu = [np.zeros((127, 344, 344), np.float32)] * 2
+    with pytest.raises(NotImplementedError, match='scatter'):
+        mmrrec.osemone({}, mu, hst, params, recmod=3)
+    with pytest.raises(ValueError, match='sctsino'):
+        mmrrec.osemone({}, mu, hst, params, recmod=2)
+    with pytest.raises(NotImplementedError, match='NIfTI'):
+        mmrrec.osemone({}, mu, hst, params, recmod=1, store_img=True)
+    with pytest.raises(NotImplementedError, match='span-11'):
+        mmrrec.osemone({}, mu, hst, dict(params, Cnt=dict(params['Cnt'], SPN=1)), recmod=1)
+    with pytest.raises(NotImplementedError, match='tAffine'):
+        pipe.mmrchain({}, params, tAffine=[np.eye(4)])
+    with pytest.raises(NotImplementedError, match='partial-volume'):
+        pipe.mmrchain({}, params, trim=True)
+    with pytest.raises(NotImplementedError, match='NIfTI'):
+        pipe.mmrchain({}, params, store_img=True)
+    with pytest.raises(NotImplementedError, match='NIfTI'):
+        pipe._mu('mumap.nii.gz')
