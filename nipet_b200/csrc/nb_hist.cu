@@ -14,11 +14,17 @@
 // per-second counters are warp-aggregated before their atomic.
 //
 // Bootstrap: the reference draws from clock()-seeded curand states; here every draw is
-// Philox4x32-10 (Salmon et al., SC'11) keyed by the 64-bit seed, with counter
-// (word index, replicate, draw), so replicates are reproducible and independent of
-// the launch shape.  btp=2 draws N ~ Poisson(btprt) per word by integer inverse CDF
-// (events with N = 0 or N >= 32 are dropped as in the reference); btp=1 replaces each
-// event word by a uniformly drawn event word of the same slice (at most 64 draws).
+// Philox4x32-10 (Salmon et al., SC'11) keyed by the 64-bit seed, so replicates are
+// reproducible and independent of the launch shape.  btp=2 draws N ~ Poisson(btprt) per
+// word by integer inverse CDF (events with N = 0 or N >= 32 are dropped as in the
+// reference) from output rep % 4 of the block with counter (word index, rep / 4, 0);
+// btp=1 replaces each event word by a uniformly drawn event word of the same slice (at
+// most 64 draws, counter (word index, replicate, 1 + draw)).
+//
+// Performance: persistent warps pull slices from a counter; per-second sums stay in
+// shared memory until the warp's second changes; with replicates the sinogram and SSRB
+// counters are replicate-interleaved ([bin][nrep], in a scratch added into the caller's
+// arrays afterwards) so one event's replicate updates fall in one or two L2 sectors.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -55,6 +61,8 @@ struct HistArgs {
   size_t nbins, sne;
   uint32_t *psino, *ssrb, *phc, *dhc, *pvs, *fan, *bck;
   int32_t *zR, *zM;
+  int ilv;                  // psino / ssrb replicate-interleaved ([bin][nrep])
+  unsigned *next_slice;     // work counter, 0 at launch
 };
 
 static __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
@@ -79,16 +87,116 @@ static __device__ __forceinline__ uint32_t boot_draw(uint64_t seed, int rep, uin
   return c[0];
 }
 
-__global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
+// one event word decoded: span-1 address parts and the histogram addresses
+struct EvDec {
+  size_t addr;   // bin of the output sinogram
+  int aw, an, w, si, sis;
+  bool valid, prompt;
+};
+
+static __device__ __forceinline__ EvDec decode_event(int word, const HistLUT &slut, int span) {
+  EvDec e;
+  const int val = word & 0x3fffffff;
+  e.si = val / NB_NSBINANG;
+  e.valid = word > 0 && e.si < NB_NSN1;
+  e.prompt = (word >> 30) == 1;
+  e.aw = e.an = e.w = e.sis = 0;
+  e.addr = 0;
+  if (e.valid) {
+    e.aw = val - e.si * NB_NSBINANG;
+    e.an = e.aw / NB_NSBINS;
+    e.w = e.aw - e.an * NB_NSBINS;
+    e.sis = slut.sn1_ssrb[e.si];
+    if (span == 1)
+      e.addr = (size_t)val;
+    else if (span == 11)
+      e.addr = (size_t)slut.sn1_sn11[e.si] * NB_NSBINANG + e.aw;
+    else
+      e.addr = (size_t)e.sis * NB_NSBINANG + e.aw;
+  }
+  return e;
+}
+
+// Add a warp's per-second sums (held per replicate in shared memory) to the global
+// per-second counters and clear them.  Lane l handles replicates l, l + 32, ...
+static __device__ __forceinline__ void flush_seconds(const HistArgs &a, uint32_t *acc, int sec,
+                                                     int lane) {
+  __syncwarp();
+  if (sec >= 0) {
+    for (int r = lane; r < a.nrep; r += 32) {
+      uint32_t *q = acc + 3 * r;
+      const uint32_t pd = q[0], sz = q[1], sd = q[2];
+      const uint32_t sp = pd;
+      const size_t o = (size_t)r * a.nitag + sec;
+      if (sp) {
+        atomicAdd(a.phc + o, sp);
+        atomicAdd((uint32_t *)a.zM + o, sp);
+        atomicAdd((uint32_t *)a.zR + o, sz);
+      }
+      if (sd) atomicAdd(a.dhc + o, sd);
+      q[0] = q[1] = q[2] = 0;
+    }
+  }
+  __syncwarp();
+}
+
+// A step's per-second sums of replicate r: into the warp's accumulators when the step lies
+// in one second (`uni`), else one global atomic per distinct second of the step.
+static __device__ __forceinline__ void second_sums(const HistArgs &a, uint32_t *acc, int r,
+                                                   bool uni, bool ok, int itag, uint32_t p_n,
+                                                   uint32_t d_n, uint32_t zr, int lane) {
+  if (uni) {
+    // prompts and delayeds of the step (each <= 31 x 32) share one reduction
+    const uint32_t spd = __reduce_add_sync(0xffffffffu, p_n | (d_n << 16));
+    const uint32_t sz = __reduce_add_sync(0xffffffffu, zr);
+    if (lane == 0) {
+      acc[3 * r] += spd & 0xFFFFu;
+      acc[3 * r + 1] += sz;
+      acc[3 * r + 2] += spd >> 16;
+    }
+    return;
+  }
+  const unsigned grp = __match_any_sync(0xffffffffu, ok ? itag : -1);
+  if (ok) {
+    const uint32_t sp = __reduce_add_sync(grp, p_n);
+    const uint32_t sd = __reduce_add_sync(grp, d_n);
+    const uint32_t sz = __reduce_add_sync(grp, zr);
+    if (lane == __ffs(grp) - 1) {
+      const size_t o = (size_t)r * a.nitag + itag;
+      if (sp) {
+        atomicAdd(a.phc + o, sp);
+        atomicAdd((uint32_t *)a.zM + o, sp);
+        atomicAdd((uint32_t *)a.zR + o, sz);
+      }
+      if (sd) atomicAdd(a.dhc + o, sd);
+    }
+  }
+}
+
+// Persistent: every warp takes the next thread slice from a.next_slice until none is left.
+// Dynamic shared memory: 3 x nrep uint32 per warp (per-second prompt, ring-sum and
+// delayed accumulators of the second the warp is in).
+__global__ void __launch_bounds__(256, 6) k_hist(const HistArgs a) {
   __shared__ HistLUT slut;
+  __shared__ uint64_t s_thr[32];
+  extern __shared__ uint32_t s_acc[];
   for (int i = threadIdx.x; i < (int)(sizeof(HistLUT) / 4); i += blockDim.x)
     reinterpret_cast<int *>(&slut)[i] = reinterpret_cast<const int *>(a.lut)[i];
+  if (threadIdx.x < 32) s_thr[threadIdx.x] = a.thr[threadIdx.x];
+  const int lane = threadIdx.x & 31;
+  uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * a.nrep;
+  for (int r = lane; r < 3 * a.nrep; r += 32) acc[r] = 0;
   __syncthreads();
 
-  const int lane = threadIdx.x & 31;
-  const int nwarps_total = (gridDim.x * blockDim.x) >> 5;
   const int nslices = a.nchnk * NB_TOTHRDS;
-  for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices; sl += nwarps_total) {
+  // replicate / bin strides of the two large counter arrays
+  const size_t pstr_r = a.ilv ? 1 : a.nbins, pstr_b = a.ilv ? (size_t)a.nrep : 1;
+  const size_t sstr_r = a.ilv ? 1 : (size_t)NB_SEG0 * NB_NSBINANG;
+  for (;;) {
+    int sl = 0;
+    if (lane == 0) sl = (int)atomicAdd(a.next_slice, 1u);
+    sl = __shfl_sync(0xffffffffu, sl, 0);
+    if (sl >= nslices) break;
     const int n = sl / NB_TOTHRDS, idx = sl - n * NB_TOTHRDS;
     const int64_t off = a.atag[n];
     const int elm = a.e4c[n], e4t = a.e4t[n];
@@ -118,13 +226,18 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
       }
     }
     const int64_t slen = s1 - s0;
+    int acc_sec = -1;  // the second whose sums `acc` holds (warp-uniform)
 
+    // the next step's words are loaded one step ahead (streaming loads: the stream is read
+    // once and should not displace the counters from L2)
+    int nxt = s0 + lane < s1 ? __ldcs(a.lm + s0 + lane) : 0;
     for (int64_t base = s0; base < s1; base += 32) {
       // a slice is dead once its current second leaves the window (hst.cu:135)
       if (!(cur >= a.tstart && cur < a.tstop)) break;
       const int64_t i = base + lane;
       const bool inb = i < s1;
-      const int word0 = inb ? a.lm[i] : 0;
+      const int word0 = nxt;  // 0 past the slice end
+      nxt = i + 32 < s1 ? __ldcs(a.lm + i + 32) : 0;
       const bool istag = inb && (word0 >> 29) == -4;
       const unsigned tmask = __ballot_sync(0xffffffffu, istag);
       const int tval = istag ? (word0 & 0x3fffffff) - a.toff : 0;
@@ -174,91 +287,132 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         }
       }
 
-      // ---- events, per replicate ----
+      // ---- events ----
+      const bool evw = live && word0 > 0;
+      const unsigned evm = __ballot_sync(0xffffffffu, evw);
+      if (evm == 0) continue;
+      // the step's second, if all its event words share one (almost every step: a
+      // second spans ~1e5 words); the per-second sums then go to the warp's accumulators
+      const int sec0 = __shfl_sync(0xffffffffu, itag, __ffs(evm) - 1);
+      const bool uni = __all_sync(0xffffffffu, !evw || itag == sec0);
+      if (uni && sec0 != acc_sec) {
+        flush_seconds(a, acc, acc_sec, lane);
+        acc_sec = sec0;
+      }
+      if (a.btp != 1) {
+        // one decode per word; per replicate only its weight N and the counter updates
+        const EvDec e = decode_event(word0, slut, a.span);
+        const bool okb = evw && e.valid;
+        const size_t pbin = e.addr * pstr_b;
+        const size_t sbin = ((size_t)e.sis * NB_NSBINANG + e.aw) * pstr_b;
+        const bool pv = okb && e.prompt && (e.an == 0 || e.an == 126) && itag < NB_MXNITAG;
+        const size_t pvo = (size_t)(itag >> 2) * NB_SEG0 * NB_NSBINS + e.sis * NB_NSBINS + e.w;
+        int f0 = 0, f1 = 0;
+        if (okb && !e.prompt) {
+          const short2 cc = a.s2cF[e.an + NB_NSANGLES * e.w];
+          f0 = NB_NCRS * slut.sn1_rno[2 * e.si] + cc.x;
+          f1 = NB_NCRS * slut.sn1_rno[2 * e.si + 1] + cc.y;
+        }
+        uint32_t blk[4] = {0u, 0u, 0u, 0u};
+        int qblk = -1;
+        for (int r = 0; r < a.nrep; r++) {
+          const int rep = a.rep0 + r;
+          uint32_t N = 1;
+          if (a.btp == 2) {
+            // N ~ Poisson: the number of inverse-CDF thresholds at or below the uniform,
+            // output rep % 4 of the Philox block (word index, rep / 4)
+            if ((rep >> 2) != qblk) {
+              qblk = rep >> 2;
+              blk[0] = (uint32_t)i;
+              blk[1] = (uint32_t)((uint64_t)i >> 32);
+              blk[2] = (uint32_t)qblk;
+              blk[3] = 0u;
+              philox4x32_10(blk, (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+            }
+            const int j = rep & 3;
+            const uint64_t x = j == 0 ? blk[0] : j == 1 ? blk[1] : j == 2 ? blk[2] : blk[3];
+            uint32_t k = 0;
+            while (k < 32 && x >= s_thr[k]) k++;
+            N = k;
+          }
+          const bool ok = okb && N > 0 && N < 32;
+          uint32_t p_n = 0, d_n = 0, zr = 0;
+          if (ok) {
+            uint32_t *ps = a.psino + (size_t)r * pstr_r + pbin;
+            if (e.prompt) {
+              p_n = N;
+              zr = (uint32_t)e.sis;
+              atomicAdd(a.ssrb + (size_t)r * sstr_r + sbin, N);
+              atomicAdd(ps, N);
+              if (pv) atomicAdd(a.pvs + (size_t)r * a.sne + pvo, N << ((e.an == 126) * 8));
+            } else {
+              d_n = N;
+              atomicAdd(ps, N << 16);
+              uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
+              atomicAdd(fn + f0, N);
+              atomicAdd(fn + f1, N);
+            }
+          }
+          second_sums(a, acc, r, uni, ok, itag, p_n, d_n, zr, lane);
+        }
+        continue;
+      }
+      // btp = 1: each replicate replaces the word by a draw from the slice
       for (int r = 0; r < a.nrep; r++) {
         const int rep = a.rep0 + r;
         int word = word0;
         uint32_t N = 1;
-        if (a.btp == 1) {
-          if (live && word0 > 0) {
-            bool got = false;
-            for (uint32_t jd = 0; jd < 64 && !got; jd++) {
-              const uint32_t x = boot_draw(a.seed, rep, (uint64_t)i, 1 + jd);
-              const int64_t bi = (int64_t)(((uint64_t)x * (uint64_t)slen) >> 32);
-              const int cand = a.lm[s0 + bi];
-              if (cand > 0) {
-                word = cand;
-                got = true;
-              }
+        if (evw) {
+          bool got = false;
+          for (uint32_t jd = 0; jd < 64 && !got; jd++) {
+            const uint32_t x = boot_draw(a.seed, rep, (uint64_t)i, 1 + jd);
+            const int64_t bi = (int64_t)(((uint64_t)x * (uint64_t)slen) >> 32);
+            const int cand = a.lm[s0 + bi];
+            if (cand > 0) {
+              word = cand;
+              got = true;
             }
-            if (!got) N = 0;
           }
-        } else if (a.btp == 2) {
-          const uint32_t x = boot_draw(a.seed, rep, (uint64_t)i, 0);
-          uint32_t k = 0;
-#pragma unroll
-          for (int q = 0; q < 32; q++) k += (uint64_t)x >= a.thr[q] ? 1u : 0u;
-          N = k;
+          if (!got) N = 0;
         }
-        const bool ev = live && word > 0 && N > 0 && N < 32;
-        const int val = word & 0x3fffffff;
-        int si = val / NB_NSBINANG;
-        const bool ok = ev && si < NB_NSN1;
+        const EvDec e = decode_event(word, slut, a.span);
+        const bool ok = evw && e.valid && N > 0;
         uint32_t p_n = 0, d_n = 0, zr = 0;
         if (ok) {
-          const int aw = val - si * NB_NSBINANG;
-          const int an = aw / NB_NSBINS;
-          const int w = aw - an * NB_NSBINS;
-          const int si11 = slut.sn1_sn11[si];
-          const int sis = slut.sn1_ssrb[si];
-          size_t addr;
-          if (a.span == 1)
-            addr = (size_t)val;
-          else if (a.span == 11)
-            addr = (size_t)si11 * NB_NSBINANG + aw;
-          else
-            addr = (size_t)sis * NB_NSBINANG + aw;
-          uint32_t *ps = a.psino + (size_t)r * a.nbins;
-          if ((word >> 30) == 1) {
+          uint32_t *ps = a.psino + (size_t)r * pstr_r + e.addr * pstr_b;
+          if (e.prompt) {
             p_n = N;
-            zr = (uint32_t)sis;
-            atomicAdd(a.ssrb + (size_t)r * NB_SEG0 * NB_NSBINANG + (size_t)sis * NB_NSBINANG + aw,
-                      N);
-            atomicAdd(ps + addr, N);
-            if ((an == 0 || an == 126) && itag < NB_MXNITAG)
+            zr = (uint32_t)e.sis;
+            atomicAdd(a.ssrb + (size_t)r * sstr_r +
+                          ((size_t)e.sis * NB_NSBINANG + e.aw) * pstr_b, N);
+            atomicAdd(ps, N);
+            if ((e.an == 0 || e.an == 126) && itag < NB_MXNITAG)
               atomicAdd(a.pvs + (size_t)r * a.sne + (size_t)(itag >> 2) * NB_SEG0 * NB_NSBINS +
-                            sis * NB_NSBINS + w,
-                        N << ((an == 126) * 8));
+                            e.sis * NB_NSBINS + e.w,
+                        N << ((e.an == 126) * 8));
           } else {
             d_n = N;
-            atomicAdd(ps + addr, N << 16);
-            const short2 cc = a.s2cF[an + NB_NSANGLES * w];
+            atomicAdd(ps, N << 16);
+            const short2 cc = a.s2cF[e.an + NB_NSANGLES * e.w];
             uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
-            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * si] + cc.x, N);
-            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * si + 1] + cc.y, N);
+            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * e.si] + cc.x, N);
+            atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * e.si + 1] + cc.y, N);
           }
         }
-        // per-second counters: one atomic per distinct second in the warp
-        const unsigned act = __ballot_sync(0xffffffffu, ok);
-        if (act) {
-          const unsigned grp = __match_any_sync(0xffffffffu, ok ? itag : -1);
-          if (ok) {
-            const uint32_t sp = __reduce_add_sync(grp, p_n);
-            const uint32_t sd = __reduce_add_sync(grp, d_n);
-            const uint32_t sz = __reduce_add_sync(grp, zr);
-            if (lane == __ffs(grp) - 1) {
-              const size_t o = (size_t)r * a.nitag + itag;
-              if (sp) {
-                atomicAdd(a.phc + o, sp);
-                atomicAdd((uint32_t *)a.zM + o, sp);
-                atomicAdd((uint32_t *)a.zR + o, sz);
-              }
-              if (sd) atomicAdd(a.dhc + o, sd);
-            }
-          }
-        }
+        second_sums(a, acc, r, uni, ok, itag, p_n, d_n, zr, lane);
       }
     }
+    flush_seconds(a, acc, acc_sec, lane);
+  }
+}
+
+// [nbins][nrep] replicate-interleaved counters added into [nrep][nbins]
+__global__ void k_deinterleave_add(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
+                                   size_t nbins, int nrep) {
+  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < nbins;
+       b += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t *s = src + b * nrep;
+    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += s[r];
   }
 }
 
@@ -365,6 +519,60 @@ static void poisson_thresholds(double lam, uint64_t thr[32]) {
   }
 }
 
+// Stream-ordered scratch of the histogrammer comes from its own memory pool per device,
+// which keeps freed memory for the next call (the replicate-interleaved counters of a
+// bootstrap run are gigabytes; re-mapping them on every call would cost more than the
+// histogram).  The pool is created on first use and lives until the process exits.
+#include <mutex>
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64] = {};
+
+static cudaError_t hist_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    g_pool[dev] = p;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+// Launch the persistent histogram kernel: as many 256-thread blocks as fit on the device at
+// once, each warp pulling thread slices from the counter `ctr` (zeroed here).
+static cudaError_t launch_hist(HistArgs &a, unsigned *ctr, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  a.next_slice = ctr;
+  const size_t dyn = (size_t)8 * 3 * a.nrep * sizeof(uint32_t);
+  int dev = 0, nsm = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (dyn > 48 * 1024) {
+    e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+  }
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist, 256, dyn);
+  if (e != cudaSuccess) return e;
+  const int nslices = a.nchnk * NB_TOTHRDS;
+  int blocks = nsm * (per_sm > 0 ? per_sm : 1);
+  if (blocks > (nslices + 7) / 8) blocks = (nslices + 7) / 8;
+  k_hist<<<blocks, 256, dyn, s>>>(a);
+  return cudaGetLastError();
+}
+
 extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag,
                        const int *ele4chnk, const int *ele4thrd, int toff, int nitag, int tstart,
                        int tstop, int span, int btp, double btprt, uint64_t seed, int rep0,
@@ -378,7 +586,7 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
              "nb_hist: NULL output");
   NB_REQUIRE(span == 0 || span == 1 || span == 11, "nb_hist: span must be 0, 1 or 11");
   NB_REQUIRE(btp >= 0 && btp <= 2, "nb_hist: btp must be 0, 1 or 2");
-  NB_REQUIRE(nrep >= 1 && nitag > 0 && nchnk >= 0, "nb_hist: bad sizes");
+  NB_REQUIRE(nrep >= 1 && nrep <= 1024 && nitag > 0 && nchnk >= 0, "nb_hist: bad sizes");
   NB_REQUIRE(!(btp == 2 && !(btprt > 0)), "nb_hist: btprt must be > 0");
   for (int n = 0; n < nchnk; n++) {
     NB_REQUIRE(atag[n] >= 0 && ele4chnk[n] >= 0 && atag[n] + ele4chnk[n] <= ele,
@@ -419,7 +627,7 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   a.fan = fan;
   a.bck = bck;
 
-  // small device-side tables, stream-ordered
+  // small device-side tables and the work counter, stream-ordered
   HistLUT hl;
   memcpy(hl.sn1_sn11, sn1_sn11, sizeof(hl.sn1_sn11));
   memcpy(hl.sn1_ssrb, sn1_ssrb, sizeof(hl.sn1_ssrb));
@@ -428,7 +636,9 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   const size_t s2c_bytes = (size_t)NB_NSBINANG * sizeof(short2);
   const size_t tot = sizeof(HistLUT) + s2c_bytes + plan_bytes + 64;
   unsigned char *d = nullptr;
-  NB_CUDA(cudaMallocAsync((void **)&d, tot, s));
+  cudaMemPool_t pool = nullptr;
+  NB_CUDA(hist_pool(&pool));
+  NB_CUDA(cudaMallocFromPoolAsync((void **)&d, tot, pool, s));
   std::vector<unsigned char> h(tot);
   size_t o = 0;
   memcpy(&h[o], &hl, sizeof(HistLUT));
@@ -447,18 +657,36 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   memcpy(&h[o], ele4thrd, sizeof(int) * nchnk);
   a.e4t = (const int *)(d + o);
   o += sizeof(int) * nchnk;
+  o = (o + 15) & ~(size_t)15;
+  unsigned *ctr = (unsigned *)(d + o);
   cudaError_t e = cudaMemcpyAsync(d, h.data(), o, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) {
+  // replicates: the two large counter arrays are histogrammed replicate-interleaved
+  // ([bin][nrep], one event's replicate updates in one or two 32-byte sectors) in a
+  // stream-ordered scratch, then added into the caller's [nrep][bin] arrays
+  uint32_t *ilv = nullptr;
+  const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
+  if (e == cudaSuccess && nrep > 1) {
+    e = cudaMallocFromPoolAsync((void **)&ilv, sizeof(uint32_t) * (a.nbins + nss) * nrep, pool,
+                                s);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(ilv, 0, sizeof(uint32_t) * (a.nbins + nss) * nrep, s);
+    if (e == cudaSuccess) {
+      a.ilv = 1;
+      a.psino = ilv;
+      a.ssrb = ilv + a.nbins * nrep;
+    }
+  }
+  if (e == cudaSuccess) e = launch_hist(a, ctr, s);
+  if (e == cudaSuccess && a.ilv) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int nslices = nchnk * NB_TOTHRDS;
-    int blocks = (nslices + 7) / 8;
-    if (blocks > nsm * 8) blocks = nsm * 8;
-    k_hist<<<blocks, 256, 0, s>>>(a);
+    k_deinterleave_add<<<nsm * 8, 256, 0, s>>>(psino, a.psino, a.nbins, nrep);
+    k_deinterleave_add<<<nsm * 8, 256, 0, s>>>(ssrb, a.ssrb, nss, nrep);
     e = cudaGetLastError();
   }
   // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go
+  if (ilv) cudaFreeAsync(ilv, s);
   cudaFreeAsync(d, s);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist", __FILE__, __LINE__);
   return NB_OK;
@@ -531,7 +759,8 @@ constexpr size_t kS2cOff = (sizeof(HistLUT) + 255) & ~(size_t)255;
 constexpr size_t kAtagOff = (kS2cOff + (size_t)NB_NSBINANG * sizeof(short2) + 255) & ~(size_t)255;
 constexpr size_t kE4cOff = kAtagOff + sizeof(int64_t) * NB_HIST_STATIC_MAX_CHUNKS;
 constexpr size_t kE4tOff = kE4cOff + sizeof(int) * NB_HIST_STATIC_MAX_CHUNKS;
-constexpr size_t kStaticEnd = kE4tOff + sizeof(int) * NB_HIST_STATIC_MAX_CHUNKS;
+constexpr size_t kCtrOff = (kE4tOff + sizeof(int) * NB_HIST_STATIC_MAX_CHUNKS + 15) & ~(size_t)15;
+constexpr size_t kStaticEnd = kCtrOff + 16;
 static_assert(kStaticEnd <= NB_HIST_STATIC_BYTES, "static histogram scratch too small");
 
 std::mutex g_static_mu;
@@ -572,7 +801,8 @@ extern "C" int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const i
              "nb_hist_static: NULL output");
   NB_REQUIRE(span == 0 || span == 1 || span == 11, "nb_hist_static: span must be 0, 1 or 11");
   NB_REQUIRE(btp >= 0 && btp <= 2, "nb_hist_static: btp must be 0, 1 or 2");
-  NB_REQUIRE(nrep >= 1 && nitag > 0 && nchnk >= 0, "nb_hist_static: bad sizes");
+  NB_REQUIRE(nrep >= 1 && nrep <= 1024 && nitag > 0 && nchnk >= 0,
+             "nb_hist_static: bad sizes");
   NB_REQUIRE(!(btp == 2 && !(btprt > 0)), "nb_hist_static: btprt must be > 0");
   if (nchnk > NB_HIST_STATIC_MAX_CHUNKS) {
     nb_set_error_msg("nb_hist_static: the chunk plan has %d chunks, but the static scratch holds "
@@ -644,16 +874,7 @@ extern "C" int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const i
     e = cudaMemcpyAsync(base + kE4cOff, ele4chnk, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(base + kE4tOff, ele4thrd, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) {
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int nslices = nchnk * NB_TOTHRDS;
-    int blocks = (nslices + 7) / 8;
-    if (blocks > nsm * 8) blocks = nsm * 8;
-    k_hist<<<blocks, 256, 0, s>>>(a);
-    e = cudaGetLastError();
-  }
+  if (e == cudaSuccess) e = launch_hist(a, reinterpret_cast<unsigned *>(base + kCtrOff), s);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist_static", __FILE__, __LINE__);
   return NB_OK;
 }

@@ -2,6 +2,7 @@
 
     python -m nipet_b200.profile_cases projectors   # k_project: back, forward, fused OSEM
     python -m nipet_b200.profile_cases hist         # k_hist on a 20M-word stream
+    python -m nipet_b200.profile_cases hist200      # k_hist on the 2e8-word, 600 s stream
 
 `projectors` builds the geometry, a phantom image (col128 layout), subset 3 of 14 and random
 prompt / (r+s)/(an) / a*n sinograms (~0.8 GB on the device), then launches the back projection
@@ -11,7 +12,8 @@ launches 15, 16, 17 are one warm launch of each mode:
     ncu --set full --clock-control none -k regex:k_project -s 15 -c 3 -o prof \\
         python -m nipet_b200.profile_cases projectors
 
-`hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2).
+`hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2);
+`hist200` does the same on the full-size 2e8-word stream over 600 s (1.2 GB on the device).
 
 `batch` runs one batched OSEM sub-iteration (subset 0) for 8 images with batch widths 4 and
 2, twice each (capture -k regex:k_osem_batch -s 2 -c 2 for the second launch of each width:
@@ -57,11 +59,11 @@ def projectors(device='cuda:0'):
     print('projectors ok')
 
 
-def hist(device='cuda:0'):
+def hist(device='cuda:0', nwords=20_000_000, duration=60):
     from . import geometry, mmr_lmproc, phantoms
     dev = torch.device(device)
     p = geometry.get_mmrparams()
-    lm = phantoms.lm_stream_fast(20_000_000, 60, params=p, seed=0, device=dev)
+    lm = phantoms.lm_stream_fast(nwords, duration, params=p, seed=0, device=dev)
     pl = mmr_lmproc.plan(lm.cpu().numpy())
     Cnt = dict(p['Cnt'], SPN=11, BTP=0)
     for _ in range(3):
@@ -94,4 +96,6 @@ def batch(device='cuda:0'):
 
 
 if __name__ == '__main__':
-    {'projectors': projectors, 'hist': hist, 'batch': batch}[sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
+    {'projectors': projectors, 'hist': hist, 'batch': batch,
+     'hist200': lambda: hist(nwords=200_000_000, duration=600)}[
+        sys.argv[1] if len(sys.argv) > 1 else 'projectors']()

@@ -651,6 +651,16 @@ static inline uint32_t boot_draw(uint64_t seed, int rep, uint64_t gidx, uint32_t
   return o[0];
 }
 
+/* Poisson bootstrap uniform of replicate `rep` for word `gidx`: output rep % 4 of the
+ * Philox block with counter (gidx, rep / 4, 0) -- one block serves four replicates. */
+static inline uint32_t boot_draw_pois(uint64_t seed, int rep, uint64_t gidx) {
+  uint32_t ctr[4] = {(uint32_t)gidx, (uint32_t)(gidx >> 32), (uint32_t)rep >> 2, 0u};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t o[4];
+  orc_philox4x32(ctr, key, o);
+  return o[rep & 3];
+}
+
 /* ========================================================================
  * List-mode chunk plan (lmaux.cu:17-226) and time-window selection
  * (lmaux.cu:229-270).  Arrays are caller-allocated with capacity `cap`.
@@ -803,7 +813,7 @@ void orc_hist(const int32_t *lm, int nchnk, const int64_t *atag, const int *ele4
             if (!got) N = 0;
           }
         } else if (btp == 2) {
-          uint32_t x = boot_draw(seed, rep, (uint64_t)i, 0);
+          uint32_t x = boot_draw_pois(seed, rep, (uint64_t)i);
           uint32_t k = 0;
           while (k < 32 && (uint64_t)x >= thr[k]) k++;
           N = k;
