@@ -176,13 +176,18 @@ static __device__ __forceinline__ void second_sums(const HistArgs &a, uint32_t *
 // Persistent: every warp takes the next thread slice from a.next_slice until none is left.
 // Dynamic shared memory: 3 x nrep uint32 per warp (per-second prompt, ring-sum and
 // delayed accumulators of the second the warp is in).
-__global__ void __launch_bounds__(256, 6) k_hist(const HistArgs a) {
+__global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   __shared__ HistLUT slut;
   __shared__ uint64_t s_thr[32];
   extern __shared__ uint32_t s_acc[];
   for (int i = threadIdx.x; i < (int)(sizeof(HistLUT) / 4); i += blockDim.x)
     reinterpret_cast<int *>(&slut)[i] = reinterpret_cast<const int *>(a.lut)[i];
   if (threadIdx.x < 32) s_thr[threadIdx.x] = a.thr[threadIdx.x];
+  // the first four Poisson thresholds in registers when none is saturated at 2^32 (they
+  // then decide almost every draw)
+  const bool fast4 = a.thr[3] < 4294967296ull;
+  const uint4 t4 = make_uint4((uint32_t)a.thr[0], (uint32_t)a.thr[1], (uint32_t)a.thr[2],
+                              (uint32_t)a.thr[3]);
   const int lane = threadIdx.x & 31;
   uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * a.nrep;
   for (int r = lane; r < 3 * a.nrep; r += 32) acc[r] = 0;
@@ -313,6 +318,10 @@ __global__ void __launch_bounds__(256, 6) k_hist(const HistArgs a) {
           f0 = NB_NCRS * slut.sn1_rno[2 * e.si] + cc.x;
           f1 = NB_NCRS * slut.sn1_rno[2 * e.si + 1] + cc.y;
         }
+        // the sinogram update of either kind, and the per-kind extra counters
+        const int pshift = e.prompt ? 0 : 16;
+        uint32_t *const ps0 = a.psino + pbin;
+        uint32_t *const ss0 = a.ssrb + sbin;
         uint32_t blk[4] = {0u, 0u, 0u, 0u};
         int qblk = -1;
         for (int r = 0; r < a.nrep; r++) {
@@ -330,30 +339,35 @@ __global__ void __launch_bounds__(256, 6) k_hist(const HistArgs a) {
               philox4x32_10(blk, (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
             }
             const int j = rep & 3;
-            const uint64_t x = j == 0 ? blk[0] : j == 1 ? blk[1] : j == 2 ? blk[2] : blk[3];
-            uint32_t k = 0;
-            while (k < 32 && x >= s_thr[k]) k++;
+            const uint32_t x = j == 0 ? blk[0] : j == 1 ? blk[1] : j == 2 ? blk[2] : blk[3];
+            uint32_t k;
+            if (fast4) {
+              k = (uint32_t)(x >= t4.x) + (uint32_t)(x >= t4.y) + (uint32_t)(x >= t4.z) +
+                  (uint32_t)(x >= t4.w);
+              if (k == 4)
+                while (k < 32 && (uint64_t)x >= s_thr[k]) k++;
+            } else {
+              k = 0;
+              while (k < 32 && (uint64_t)x >= s_thr[k]) k++;
+            }
             N = k;
           }
           const bool ok = okb && N > 0 && N < 32;
-          uint32_t p_n = 0, d_n = 0, zr = 0;
           if (ok) {
-            uint32_t *ps = a.psino + (size_t)r * pstr_r + pbin;
+            atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
             if (e.prompt) {
-              p_n = N;
-              zr = (uint32_t)e.sis;
-              atomicAdd(a.ssrb + (size_t)r * sstr_r + sbin, N);
-              atomicAdd(ps, N);
+              atomicAdd(ss0 + (size_t)r * sstr_r, N);
               if (pv) atomicAdd(a.pvs + (size_t)r * a.sne + pvo, N << ((e.an == 126) * 8));
             } else {
-              d_n = N;
-              atomicAdd(ps, N << 16);
               uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
               atomicAdd(fn + f0, N);
               atomicAdd(fn + f1, N);
             }
           }
-          second_sums(a, acc, r, uni, ok, itag, p_n, d_n, zr, lane);
+          // centre of mass: zR adds the prompt's SSRB index once, zM its weight (hst.cu:176-178)
+          const uint32_t nn = ok ? N : 0u;
+          second_sums(a, acc, r, uni, ok, itag, e.prompt ? nn : 0u, e.prompt ? 0u : nn,
+                      (ok && e.prompt) ? (uint32_t)e.sis : 0u, lane);
         }
         continue;
       }

@@ -3,6 +3,7 @@
     python -m nipet_b200.profile_cases projectors   # k_project: back, forward, fused OSEM
     python -m nipet_b200.profile_cases hist         # k_hist on a 20M-word stream
     python -m nipet_b200.profile_cases hist200      # k_hist on the 2e8-word, 600 s stream
+    python -m nipet_b200.profile_cases hist200boot  # the same with 4 Poisson replicates
 
 `projectors` builds the geometry, a phantom image (col128 layout), subset 3 of 14 and random
 prompt / (r+s)/(an) / a*n sinograms (~0.8 GB on the device), then launches the back projection
@@ -13,7 +14,9 @@ launches 15, 16, 17 are one warm launch of each mode:
         python -m nipet_b200.profile_cases projectors
 
 `hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2);
-`hist200` does the same on the full-size 2e8-word stream over 600 s (1.2 GB on the device).
+`hist200` does the same on the full-size 2e8-word stream over 600 s (1.2 GB on the device);
+`hist200boot` histograms that stream with 4 Poisson bootstrap replicates per launch (about
+3.4 GB on the device).
 
 `batch` runs one batched OSEM sub-iteration (subset 0) for 8 images with batch widths 4 and
 2, twice each (capture -k regex:k_osem_batch -s 2 -c 2 for the second launch of each width:
@@ -59,17 +62,19 @@ def projectors(device='cuda:0'):
     print('projectors ok')
 
 
-def hist(device='cuda:0', nwords=20_000_000, duration=60):
+def hist(device='cuda:0', nwords=20_000_000, duration=60, nrep=1):
     from . import geometry, mmr_lmproc, phantoms
     dev = torch.device(device)
     p = geometry.get_mmrparams()
     lm = phantoms.lm_stream_fast(nwords, duration, params=p, seed=0, device=dev)
     pl = mmr_lmproc.plan(lm.cpu().numpy())
-    Cnt = dict(p['Cnt'], SPN=11, BTP=0)
+    Cnt = dict(p['Cnt'], SPN=11, BTP=0 if nrep == 1 else 2, BTPRT=1.0)
     for _ in range(3):
-        r = mmr_lmproc.hist_stream(lm, p['txLUT'], p['axLUT'], Cnt, pl=pl, unpack=False)
+        r = mmr_lmproc.hist_stream(lm, p['txLUT'], p['axLUT'], Cnt, pl=pl, unpack=False,
+                                   nrep=nrep)
     torch.cuda.synchronize(dev)
     print('hist ok', int(r['phc'].sum()))
+    del r
 
 
 def batch(device='cuda:0'):
@@ -97,5 +102,6 @@ def batch(device='cuda:0'):
 
 if __name__ == '__main__':
     {'projectors': projectors, 'hist': hist, 'batch': batch,
-     'hist200': lambda: hist(nwords=200_000_000, duration=600)}[
+     'hist200': lambda: hist(nwords=200_000_000, duration=600),
+     'hist200boot': lambda: hist(nwords=200_000_000, duration=600, nrep=4)}[
         sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
