@@ -1,7 +1,7 @@
 """Benchmark of the mMR reconstruction hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batch|osem|hist] [--replicates R]
+                    [--workload batch|osem|hist|diff|dynamic] [--replicates R]
 
 Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand in for):
   batch (default) batched bootstrap OSEM: R = 50 Poisson replicates of one synthetic scan
@@ -11,7 +11,11 @@ Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand
         graph per iteration.  Metric: reconstructions (replicates) per second.
   osem  one plain OSEM reconstruction per step (same scan: brain phantom, water
         attenuation, log-normal crystal efficiencies, 20% uniform randoms, 3e7 counts).
-  hist  list-mode histogramming of a synthetic 32-bit mMR event stream (events/s).
+  hist  list-mode histogramming of a synthetic 32-bit mMR event stream: span 11, span 1 and
+        10 Poisson bootstrap replicates per step (events/s).
+  diff  differentiable projector: 8 images, forward projection with attenuation x norm,
+        Poisson NLL and its gradient through the back projector (images/s).
+  dynamic  16 span-1 frames reconstructed batched, then each frame's NLL gradient (frames/s).
 
 `value` is measured on device-resident inputs (CUDA events, barrier + synchronize on
 both sides; inputs larger than L2, or L2 flushed between steps); `e2e` times the public
@@ -583,10 +587,29 @@ def run_dynamic(args, ws, rank, dev):
     scan = dynamic.dynamic_scan(params, dev, counts, seed=rank)
     dyn = dynamic.DynamicRecon(params, scan)
     nfr = dyn.nframes
+    br = dyn.rec
 
-    def step():
-        dyn.run(niter=4)
+    def step(ev=None):
+        # DynamicRecon.run(niter=4), with the iterations bracketed by events when timed
+        br.sensitivity()
+        br.init_images()
+        for _ in range(4):
+            if ev is not None:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+            br.iteration(use_graph=True)
+            if ev is not None:
+                e1.record()
+                ev.append((e0, e1))
         return dyn.nll_gradients()
+
+    # per-launch algorithmic bytes of k_osem_batch at span 1 (as in the batch workload:
+    # 8 B per voxel read/update per frame, prompt rows and one (r+s)/(an), a*n row per group)
+    _, per_lor = br.geom.count_reads(per_lor=True)
+    ngroups = (nfr + br.bs - 1) // br.bs
+    bytes_iter = float(sum(nfr * 8 * int(per_lor[sb.cpu().numpy()].sum()) +
+                           br.nprj * 4084 * (2 * nfr + 8 * ngroups) for sb in br.subs))
 
     for _ in range(args.warmup):
         step()
@@ -594,19 +617,46 @@ def run_dynamic(args, ws, rank, dev):
     dyn.rec.launches = 0
     dyn.launches = 0
     clk = Clocks(dev.index) if rank == 0 else None
-    times = []
+    times, it_ms = [], []
     for _ in range(args.steps):
         _barrier(ws, dev)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        step()
+        ev = []
+        step(ev)
         t1.record()
         _barrier(ws, dev)
         times.append(t0.elapsed_time(t1) / 1e3)
+        it_ms += [a.elapsed_time(b) for a, b in ev]
     clocks = clk.stop() if clk else None
     dyn.rec.geom.check()
     t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    t_it = float(np.mean(it_ms)) / 1e3
+    achieved = bytes_iter / t_it / 1e9
+    peak, peak_kind = _peaks()
+    wf8 = _traffic('osem_batch_8img_smem_wavefronts')
+    onchip = None
+    if wf8:
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+        ach = wf8 * nfr / 8.0 / (t_it / len(br.subs))
+        onchip = {'bound': 'shared-memory pipe', 'unit': 'wavefronts/s', 'achieved': ach,
+                  'peak': nsm * mhz * 1e6, 'frac': ach / (nsm * mhz * 1e6),
+                  'wavefronts_per_launch': wf8 * nfr / 8.0,
+                  'peak_basis': f'1 wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz',
+                  'note': 'wavefronts of the 8-image span-11 capture scaled by frames (the '
+                          'same ray walks; span-1 sinogram rows are 4.9x longer)'}
+    roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+            'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
+            'kernel': f'k_osem_batch span 1 (nb_osem_batch_subset, {br.bs} frames per walk, '
+                      f'tile {br.tile})',
+            'bytes_per_launch_avg': bytes_iter / len(br.subs),
+            'launch_ms_avg': t_it * 1e3 / len(br.subs),
+            'note': 'achieved counts 4 B per Siddon voxel read/update as if from HBM; the '
+                    'kernel serves them from shared memory (see onchip); traffic: no span-1 '
+                    'capture',
+            'onchip': onchip}
     # e2e: pinned host prompts in, host frames and gradients out
     ph = scan['psng'].cpu().pin_memory()
     img_h = torch.empty((nfr, 320, 320, 127)).pin_memory()
@@ -633,7 +683,7 @@ def run_dynamic(args, ws, rank, dev):
                    'd2h_bytes_per_step': int(2 * img_h.numel() * 4)},
            'clocks': clocks,
            'gpu_launches': (dyn.rec.launches + dyn.launches) // max(1, args.steps),
-           'roofline': None,
+           'roofline': roof,
            'config': {'workload': f'span-1 dynamic: {nfr} frames '
                                   f'({counts.min():.0e}..{counts.max():.0e} counts), 4084 '
                                   'sinograms, 320x320x127, 4 it x 14 subsets batched, per-frame '
