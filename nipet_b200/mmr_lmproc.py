@@ -73,14 +73,16 @@ def plan(lm: np.ndarray, t0: int = 0, t1: int = 0) -> dict:
 
 def hist_stream(lm, txLUT: dict, axLUT: dict, Cnt: dict, t0: int = 0, t1: int = 0,
                 nrep: int = 1, rep0: int = 0, seed: int = 0, lm_host: np.ndarray | None = None,
-                pl: dict | None = None, device=None, unpack: bool = True) -> dict:
+                pl: dict | None = None, device=None, unpack: bool = True,
+                events: list | None = None) -> dict:
     """Histogram a list-mode word stream on the GPU.
 
     `lm`: host numpy int32 words or a device tensor; the chunk plan needs the words on
     the host (`lm_host`, or `lm` itself when it is a numpy array) unless `pl` is given.
     Returns device tensors (a leading replicate axis when nrep > 1): `psino` (packed),
     `psn`/`dsn` (uint16, if `unpack`), `ssr`, `phc`, `dhc`, `mss`, `pvs`, `fan`, `bck`,
-    and `psum`/`dsum` totals of replicate 0."""
+    and `psum`/`dsum` totals of replicate 0.  `events`, if a list, receives a pair of
+    recorded CUDA events around the histogram launch (`nb_hist`) alone."""
     dev = device_of(Cnt, device)
     span = int(Cnt['SPN'])
     if span not in NBINS:
@@ -109,12 +111,18 @@ def hist_stream(lm, txLUT: dict, axLUT: dict, Cnt: dict, t0: int = 0, t1: int = 
     atag = np.ascontiguousarray(pl['atag'], dtype=np.int64)
     e4c = np.ascontiguousarray(pl['ele4chnk'], dtype=np.int32)
     e4t = np.ascontiguousarray(pl['ele4thrd'], dtype=np.int32)
+    if events is not None:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(torch.cuda.current_stream(dev))
     _lib.check(_lib.load().nb_hist(
         dev_ptr(d_lm), d_lm.numel(), pl['nchnk'], hp(atag), hp(e4c), hp(e4t),
         pl['toff'], nitag, pl['tstart'], pl['tstop'], span, btp, btprt, int(seed), int(rep0),
         int(nrep), *[hp(a) for a in luts], dev_ptr(out['psino']), dev_ptr(out['ssr']),
         dev_ptr(out['phc']), dev_ptr(out['dhc']), dev_ptr(out['zR']), dev_ptr(out['zM']),
         dev_ptr(out['pvs']), dev_ptr(out['fan']), dev_ptr(out['bck']), st))
+    if events is not None:
+        ev1.record(torch.cuda.current_stream(dev))
+        events.append((ev0, ev1))
     res = {k: v.view(torch.uint32) if k not in ('zR', 'zM') else v for k, v in out.items()}
     # centre of mass: zR / (float) zM per second (lmproc.cu:189-193), float division
     res['mss'] = res['zR'].to(torch.float32) / res['zM'].to(torch.float32)
