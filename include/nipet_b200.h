@@ -150,7 +150,7 @@ int nb_osem_subset_psf(nb_geom *g, float *img128, float *bimg128, const float *s
  *   sens128    dev col128 sensitivity image of this subset; msk128 dev col128 uint8 mask
  *   psng       dev [nrep][68516][nsinos] uint16 prompts; rs dev [68516][nsinos] float
  *              (r+s)/(an) from nb_osem_rs; rscale dev [nrep] per-image randoms factor
- *   bs         1, 2 or 4 (4: span 11 only); span 11 (837 sinograms) or 1 (4084)
+ *   bs         1, 2 or 4; span 11 (837 sinograms) or 1 (4084)
  *   tile       kernel shape: 0 = 1024 threads x 4 rays each, 64/bs columns of the LOR
  *              staged per shared-memory chunk; 1 = the same threads, 32/bs columns per
  *              chunk; 2 = 512 threads x 8 rays, 64/bs columns.  Results agree to rounding;

@@ -189,7 +189,7 @@ def autotune(rec: BatchRecon, candidates=None, repeats: int = 2):
     except Exception:
         disk = {}
     if candidates is None:
-        widths = [1, 2, 4] if rec.span == 11 else [1, 2]
+        widths = [1, 2, 4]
         widths = [w for w in widths if w <= max(1, rec.nrep) or w == 1]
         candidates = [(w, t) for w in widths for t in TILES]
     best, best_t = candidates[0], float('inf')

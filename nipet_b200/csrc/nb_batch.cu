@@ -651,6 +651,7 @@ template <int MODE> int launch_batch_prj(nb_geom *g, const nbb::BatchArgs &a, in
     if (bs == 2) return launch_batch<2, 32, NB_NSN11, 1024, 4, MODE>(g, a, s);
     return launch_batch<1, 64, NB_NSN11, 1024, 4, MODE>(g, a, s);
   }
+  if (bs == 4) return launch_batch<4, 8, NB_NSN1, 1024, 4, MODE>(g, a, s);
   if (bs == 2) return launch_batch<2, 32, NB_NSN1, 1024, 4, MODE>(g, a, s);
   return launch_batch<1, 64, NB_NSN1, 1024, 4, MODE>(g, a, s);
 }
@@ -685,8 +686,7 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
              "nb_osem_batch_subset: NULL argument");
   NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_osem_batch_subset: nrep out of range");
   NB_REQUIRE(span == 11 || span == 1, "nb_osem_batch_subset: span must be 1 or 11");
-  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
-             "nb_osem_batch_subset: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(bs == 1 || bs == 2 || bs == 4, "nb_osem_batch_subset: bs must be 1, 2 or 4");
   NB_REQUIRE(tile >= 0 && tile <= 2, "nb_osem_batch_subset: tile must be 0, 1 or 2");
   NB_REQUIRE(nprj > 0, "nb_osem_batch_subset: empty subset");
   NB_CUDA(cudaSetDevice(g->device));
@@ -714,7 +714,11 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
     else
       st = NB_TILES(1, 64, NB_NSN11);
   } else {
-    if (bs == 2)
+    // span 1: a LOR's ratio rows are 4084 x bs floats, so 4 images stage 8 columns per
+    // chunk (16 would need 257 KB of shared memory)
+    if (bs == 4)
+      st = NB_TILES(4, 8, NB_NSN1);
+    else if (bs == 2)
       st = NB_TILES(2, 32, NB_NSN1);
     else
       st = NB_TILES(1, 64, NB_NSN1);
@@ -738,8 +742,7 @@ extern "C" int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep
   NB_REQUIRE(sino && img, "nb_fprj_batch: NULL argument");
   NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_fprj_batch: nrep out of range");
   NB_REQUIRE(span == 11 || span == 1, "nb_fprj_batch: span must be 1 or 11");
-  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
-             "nb_fprj_batch: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(bs == 1 || bs == 2 || bs == 4, "nb_fprj_batch: bs must be 1, 2 or 4");
   NB_REQUIRE(nprj > 0 && (subs != nullptr || nprj == g->naw), "nb_fprj_batch: bad subset");
   NB_CUDA(cudaSetDevice(g->device));
   nbb::BatchArgs a{};
@@ -755,8 +758,7 @@ extern "C" int nb_bprj_batch(nb_geom *g, float *bimg, const float *sino, int nre
   NB_REQUIRE(sino && bimg, "nb_bprj_batch: NULL argument");
   NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_bprj_batch: nrep out of range");
   NB_REQUIRE(span == 11 || span == 1, "nb_bprj_batch: span must be 1 or 11");
-  NB_REQUIRE(bs == 1 || bs == 2 || (bs == 4 && span == 11),
-             "nb_bprj_batch: bs must be 1, 2 or (span 11) 4");
+  NB_REQUIRE(bs == 1 || bs == 2 || bs == 4, "nb_bprj_batch: bs must be 1, 2 or 4");
   NB_REQUIRE(nprj > 0 && (subs != nullptr || nprj == g->naw), "nb_bprj_batch: bad subset");
   NB_CUDA(cudaSetDevice(g->device));
   nbb::BatchArgs a{};

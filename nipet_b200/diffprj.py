@@ -76,8 +76,8 @@ class MMRProjector:
         return dev_ptr(self.subs) if self.subs is not None else None
 
     def _width(self, nimg: int) -> int:
-        """Images per walk of the geometry for a batch of nimg (1, 2 or, at span 11, 4)."""
-        if nimg >= 4 and self.span == 11:
+        """Images per walk of the geometry for a batch of nimg (1, 2 or 4)."""
+        if nimg >= 4:
             return 4
         return 2 if nimg >= 2 else 1
 

@@ -93,7 +93,7 @@ class DynamicRecon:
     """Batched span-1 OSEM of all frames of a `dynamic_scan`, then per-frame Poisson
     log-likelihood gradients through `diffprj.MMRProjector`.
 
-    bs (frames per walk of the geometry, 1 or 2 at span 1) and the kernel tile are picked
+    bs (frames per walk of the geometry: 1, 2 or 4) and the kernel tile are picked
     by the batch autotuner when None."""
 
     def __init__(self, params: dict, scan: dict, device=None, bs: int | None = None,

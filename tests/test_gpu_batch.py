@@ -82,7 +82,7 @@ def test_autotune_picks_a_valid_shape(params, scan, replicates, cuda_device, tmp
     assert (tmp_path / 'autotune.json').exists()
 
 
-@pytest.mark.parametrize('span,bs', [(11, 4), (11, 2), (11, 1), (1, 2)])
+@pytest.mark.parametrize('span,bs', [(11, 4), (11, 2), (11, 1), (1, 4), (1, 2)])
 def test_batched_projector_pair_matches_single(params, cuda_device, span, bs):
     """nb_fprj_batch / nb_bprj_batch (one walk per bs images) against nb_fprj / nb_bprj
     image by image on a 512-LOR subset: <= 1e-5 relative per bin (bins >= 1e-3 of the

@@ -40,7 +40,7 @@ def _unfused(params, scan, k, device, niter=1):
     return x
 
 
-@pytest.mark.parametrize('bs', [1, 2])
+@pytest.mark.parametrize('bs', [1, 2, 4])
 def test_span1_batch_matches_unfused_osem(params, scan, cuda_device, bs):
     dyn = dynamic.DynamicRecon(params, scan, bs=bs).run(niter=1, use_graph=False)
     got = dyn.images()
