@@ -22,9 +22,13 @@
 // most 64 draws, counter (word index, replicate, 1 + draw)).
 //
 // Performance: persistent warps pull slices from a counter; per-second sums stay in
-// shared memory until the warp's second changes; with replicates the sinogram and SSRB
-// counters are replicate-interleaved ([bin][nrep], in a scratch added into the caller's
-// arrays afterwards) so one event's replicate updates fall in one or two L2 sectors.
+// shared memory until the warp's second changes.  With bootstrap replicates nb_hist counts
+// the sinogram unpacked in a scratch ([bin][2][nrep]: prompts and delayeds apart, a bin's
+// replicates side by side, so one event's replicate updates share one or two L2
+// sectors), then packs it into the caller's sinograms (prompts + 65536 x delayeds, the
+// reference's uint32 sum) and sums the SSRB counters from the prompts (every output
+// sinogram lies in one SSRB sinogram), so the SSRB counters take no atomics.  A single
+// histogram, and nb_hist_static (which may not allocate), count both directly.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -61,7 +65,9 @@ struct HistArgs {
   size_t nbins, sne;
   uint32_t *psino, *ssrb, *phc, *dhc, *pvs, *fan, *bck;
   int32_t *zR, *zM;
-  int ilv;                  // psino / ssrb replicate-interleaved ([bin][nrep])
+  int unp;                  // 1: psino is an unpacked scratch [bin][2][nrep] (prompts,
+                            // delayeds) and SSRB is derived afterwards; 0: packed
+                            // [nrep][bin] with SSRB counted here
   unsigned *next_slice;     // work counter, 0 at launch
 };
 
@@ -195,8 +201,11 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
 
   const int nslices = a.nchnk * NB_TOTHRDS;
   // replicate / bin strides of the two large counter arrays
-  const size_t pstr_r = a.ilv ? 1 : a.nbins, pstr_b = a.ilv ? (size_t)a.nrep : 1;
-  const size_t sstr_r = a.ilv ? 1 : (size_t)NB_SEG0 * NB_NSBINANG;
+  // replicate / bin strides of the sinogram counters, the delayed slot offset and shift
+  const size_t pstr_r = a.unp ? 1 : a.nbins, pstr_b = a.unp ? 2 * (size_t)a.nrep : 1;
+  const size_t doff = a.unp ? (size_t)a.nrep : 0;
+  const int dshift = a.unp ? 0 : 16;
+  const size_t sstr_r = (size_t)NB_SEG0 * NB_NSBINANG;
   for (;;) {
     int sl = 0;
     if (lane == 0) sl = (int)atomicAdd(a.next_slice, 1u);
@@ -308,8 +317,8 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         // one decode per word; per replicate only its weight N and the counter updates
         const EvDec e = decode_event(word0, slut, a.span);
         const bool okb = evw && e.valid;
-        const size_t pbin = e.addr * pstr_b;
-        const size_t sbin = ((size_t)e.sis * NB_NSBINANG + e.aw) * pstr_b;
+        const size_t pbin = e.addr * pstr_b + (e.prompt ? 0 : doff);
+        const size_t sbin = (size_t)e.sis * NB_NSBINANG + e.aw;
         const bool pv = okb && e.prompt && (e.an == 0 || e.an == 126) && itag < NB_MXNITAG;
         const size_t pvo = (size_t)(itag >> 2) * NB_SEG0 * NB_NSBINS + e.sis * NB_NSBINS + e.w;
         int f0 = 0, f1 = 0;
@@ -319,7 +328,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           f1 = NB_NCRS * slut.sn1_rno[2 * e.si + 1] + cc.y;
         }
         // the sinogram update of either kind, and the per-kind extra counters
-        const int pshift = e.prompt ? 0 : 16;
+        const int pshift = e.prompt ? 0 : dshift;
         uint32_t *const ps0 = a.psino + pbin;
         uint32_t *const ss0 = a.ssrb + sbin;
         uint32_t blk[4] = {0u, 0u, 0u, 0u};
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           if (ok) {
             atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
             if (e.prompt) {
-              atomicAdd(ss0 + (size_t)r * sstr_r, N);
+              if (!a.unp) atomicAdd(ss0 + (size_t)r * sstr_r, N);
               if (pv) atomicAdd(a.pvs + (size_t)r * a.sne + pvo, N << ((e.an == 126) * 8));
             } else {
               uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
@@ -397,8 +406,8 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           if (e.prompt) {
             p_n = N;
             zr = (uint32_t)e.sis;
-            atomicAdd(a.ssrb + (size_t)r * sstr_r +
-                          ((size_t)e.sis * NB_NSBINANG + e.aw) * pstr_b, N);
+            if (!a.unp)
+              atomicAdd(a.ssrb + (size_t)r * sstr_r + (size_t)e.sis * NB_NSBINANG + e.aw, N);
             atomicAdd(ps, N);
             if ((e.an == 0 || e.an == 126) && itag < NB_MXNITAG)
               atomicAdd(a.pvs + (size_t)r * a.sne + (size_t)(itag >> 2) * NB_SEG0 * NB_NSBINS +
@@ -406,7 +415,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
                         N << ((e.an == 126) * 8));
           } else {
             d_n = N;
-            atomicAdd(ps, N << 16);
+            atomicAdd(ps + doff, N << dshift);
             const short2 cc = a.s2cF[e.an + NB_NSANGLES * e.w];
             uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
             atomicAdd(fn + NB_NCRS * slut.sn1_rno[2 * e.si] + cc.x, N);
@@ -420,13 +429,35 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   }
 }
 
-// [nbins][nrep] replicate-interleaved counters added into [nrep][nbins]
-__global__ void k_deinterleave_add(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
-                                   size_t nbins, int nrep) {
+// Unpacked scratch [bin][2][nrep] (prompts, delayeds) added into the caller's packed
+// [nrep][bin] counters: prompts + 65536 x delayeds, the reference's packed uint32 sum
+// (hst.cu:167,192), wrap-around included.
+__global__ void k_pack_add(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
+                           size_t nbins, int nrep) {
   for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < nbins;
        b += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t *s = src + b * nrep;
-    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += s[r];
+    const uint32_t *q = src + b * 2 * nrep;
+    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += q[r] + (q[nrep + r] << 16);
+  }
+}
+
+// SSRB counters from the unpacked prompts: every output sinogram belongs to one SSRB
+// sinogram (its rings' sum), so SSRB bin (k, aw) of replicate r adds the prompts of bin aw
+// of the sinograms listed in src[off[k] .. off[k+1]).
+__global__ void k_ssrb_derive(uint32_t *__restrict__ ssrb, const uint32_t *__restrict__ src,
+                              const int *__restrict__ off, const int16_t *__restrict__ lst,
+                              int nrep) {
+  const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nss;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i / NB_NSBINANG), aw = (int)(i - (size_t)k * NB_NSBINANG);
+    const int j0 = off[k], j1 = off[k + 1];
+    for (int r = 0; r < nrep; r++) {
+      uint32_t acc = 0;
+      for (int j = j0; j < j1; j++)
+        acc += src[((size_t)lst[j] * NB_NSBINANG + aw) * 2 * nrep + r];
+      ssrb[(size_t)r * nss + i] += acc;
+    }
   }
 }
 
@@ -641,14 +672,34 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   a.fan = fan;
   a.bck = bck;
 
-  // small device-side tables and the work counter, stream-ordered
+  // small device-side tables, the SSRB source lists and the work counter, stream-ordered
   HistLUT hl;
   memcpy(hl.sn1_sn11, sn1_sn11, sizeof(hl.sn1_sn11));
   memcpy(hl.sn1_ssrb, sn1_ssrb, sizeof(hl.sn1_ssrb));
   memcpy(hl.sn1_rno, sn1_rno, sizeof(hl.sn1_rno));
+  // SSRB sinogram k gathers the output sinograms listed in lst[off[k] .. off[k+1]): span 11
+  // its span-11 sinograms (each has one SSRB index), span 1 its span-1 sinograms, SSRB
+  // mode itself
+  const int nout = span == 11 ? NB_NSN11 : (span == 1 ? NB_NSN1 : NB_SEG0);
+  std::vector<int> ssrb_of(nout, -1);
+  for (int si = 0; si < NB_NSN1; si++) {
+    const int so = span == 11 ? sn1_sn11[si] : (span == 1 ? si : sn1_ssrb[si]);
+    const int k = span == 0 ? so : sn1_ssrb[si];
+    NB_REQUIRE(ssrb_of[so] < 0 || ssrb_of[so] == k,
+               "nb_hist: an output sinogram spans two SSRB sinograms");
+    ssrb_of[so] = k;
+  }
+  std::vector<int> soff(NB_SEG0 + 1, 0);
+  std::vector<int16_t> slst;
+  for (int k = 0; k < NB_SEG0; k++) {
+    for (int so = 0; so < nout; so++)
+      if (ssrb_of[so] == k) slst.push_back((int16_t)so);
+    soff[k + 1] = (int)slst.size();
+  }
   const size_t plan_bytes = (size_t)nchnk * (sizeof(int64_t) + 2 * sizeof(int));
   const size_t s2c_bytes = (size_t)NB_NSBINANG * sizeof(short2);
-  const size_t tot = sizeof(HistLUT) + s2c_bytes + plan_bytes + 64;
+  const size_t ssl_bytes = sizeof(int) * soff.size() + sizeof(int16_t) * slst.size();
+  const size_t tot = sizeof(HistLUT) + s2c_bytes + plan_bytes + ssl_bytes + 96;
   unsigned char *d = nullptr;
   cudaMemPool_t pool = nullptr;
   NB_CUDA(hist_pool(&pool));
@@ -672,35 +723,42 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   a.e4t = (const int *)(d + o);
   o += sizeof(int) * nchnk;
   o = (o + 15) & ~(size_t)15;
+  memcpy(&h[o], soff.data(), sizeof(int) * soff.size());
+  const int *d_soff = (const int *)(d + o);
+  o += sizeof(int) * soff.size();
+  memcpy(&h[o], slst.data(), sizeof(int16_t) * slst.size());
+  const int16_t *d_slst = (const int16_t *)(d + o);
+  o += sizeof(int16_t) * slst.size();
+  o = (o + 15) & ~(size_t)15;
   unsigned *ctr = (unsigned *)(d + o);
   cudaError_t e = cudaMemcpyAsync(d, h.data(), o, cudaMemcpyHostToDevice, s);
-  // replicates: the two large counter arrays are histogrammed replicate-interleaved
-  // ([bin][nrep], one event's replicate updates in one or two 32-byte sectors) in a
-  // stream-ordered scratch, then added into the caller's [nrep][bin] arrays
-  uint32_t *ilv = nullptr;
-  const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
+  // replicates: the sinogram counters are histogrammed unpacked -- prompts and delayeds
+  // of a bin in separate uint32s, the replicates of a bin side by side ([bin][2][nrep], so
+  // one event's replicate updates share one or two 32-byte sectors) -- in a stream-ordered
+  // scratch, then packed into the caller's sinograms, and the SSRB counters are summed
+  // from the prompts instead of counted per event.  One histogram counts both directly
+  // (an unpacked scratch would double its L2 footprint for less than it saves).
+  uint32_t *scr = nullptr;
+  const size_t scr_bytes = sizeof(uint32_t) * a.nbins * 2 * (size_t)nrep;
   if (e == cudaSuccess && nrep > 1) {
-    e = cudaMallocFromPoolAsync((void **)&ilv, sizeof(uint32_t) * (a.nbins + nss) * nrep, pool,
-                                s);
-    if (e == cudaSuccess)
-      e = cudaMemsetAsync(ilv, 0, sizeof(uint32_t) * (a.nbins + nss) * nrep, s);
+    e = cudaMallocFromPoolAsync((void **)&scr, scr_bytes, pool, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scr, 0, scr_bytes, s);
     if (e == cudaSuccess) {
-      a.ilv = 1;
-      a.psino = ilv;
-      a.ssrb = ilv + a.nbins * nrep;
+      a.unp = 1;
+      a.psino = scr;
     }
   }
   if (e == cudaSuccess) e = launch_hist(a, ctr, s);
-  if (e == cudaSuccess && a.ilv) {
+  if (e == cudaSuccess && a.unp) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    k_deinterleave_add<<<nsm * 8, 256, 0, s>>>(psino, a.psino, a.nbins, nrep);
-    k_deinterleave_add<<<nsm * 8, 256, 0, s>>>(ssrb, a.ssrb, nss, nrep);
+    k_pack_add<<<nsm * 8, 256, 0, s>>>(psino, scr, a.nbins, nrep);
+    k_ssrb_derive<<<nsm * 8, 256, 0, s>>>(ssrb, scr, d_soff, d_slst, nrep);
     e = cudaGetLastError();
   }
   // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go
-  if (ilv) cudaFreeAsync(ilv, s);
+  if (scr) cudaFreeAsync(scr, s);
   cudaFreeAsync(d, s);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist", __FILE__, __LINE__);
   return NB_OK;
