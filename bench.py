@@ -1004,7 +1004,9 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--steps', type=int, default=None,
+                    help='timed steps (default 3; 20 for our hist arm, whose step is ~60 ms, '
+                         'so that the clock record spans several samples)')
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='batch',
@@ -1016,6 +1018,8 @@ def main():
     ap.add_argument('--duration', type=int, default=600)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if (args.workload == 'hist' and args.impl == 'ours') else 3
 
     if args.impl == 'reference':
         out = run_reference(args)
