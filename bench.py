@@ -16,6 +16,9 @@ Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand
   diff  differentiable projector: 8 images, forward projection with attenuation x norm,
         Poisson NLL and its gradient through the back projector (images/s).
   dynamic  16 span-1 frames reconstructed batched, then each frame's NLL gradient (frames/s).
+  chain  one frame reconstructed from the list-mode stream through mmrrec.osemone: histogram,
+        randoms from the delayed fan sums, norm from its components, attenuation from the
+        mu-map, 14 sensitivity images, 4 x 14 OSEM (recon/s).
 
 `value` is measured on device-resident inputs (CUDA events, barrier + synchronize on
 both sides; inputs larger than L2, or L2 flushed between steps); `e2e` times the public
@@ -51,7 +54,9 @@ METRIC = {'batch': ('OSEM recon/s span-11 320\u00b2\u00d7127 (batched+autograd v
           'dynamic': ('span-1 dynamic frames/s (batched OSEM + per-frame NLL gradient)',
                       'frames/s'),
           'osem': ('OSEM recon/s span-11 320x320x127 (plain, one scan)', 'recon/s'),
-          'hist': ('list-mode histogram events/s', 'events/s')}
+          'hist': ('list-mode histogram events/s', 'events/s'),
+          'chain': ('single-frame reconstructions/s from list mode (histogram, randoms, norm, '
+                    'attenuation, sensitivity, OSEM 4x14, span-11)', 'recon/s')}
 
 
 def _peaks():
@@ -808,6 +813,116 @@ def run_hist(args, ws, rank, dev):
     return res
 
 
+
+# ---------------------------------------------------------------------------------------
+# chain: one frame from list mode through mmrrec.osemone
+# ---------------------------------------------------------------------------------------
+def _norm_components(seed=12):
+    """Seeded synthetic norm components of the norm file's shapes (no scanner file here)."""
+    rng = np.random.default_rng(seed)
+    u = lambda lo, hi, shape: rng.uniform(lo, hi, size=shape).astype(np.float32)  # noqa: E731
+    ceff = u(0.7, 1.3, (64, 504))
+    ceff[:, 8::9] = 0.0
+    return {'geo': u(0.5, 2.0, (127, 344)), 'cinf': u(0.9, 1.1, (344, 9)), 'ceff': ceff,
+            'axe1': u(0.8, 1.2, 837), 'axf1': u(0.8, 1.2, 4084),
+            'dtp': u(-3e-6, -1e-6, 64), 'dtnp': u(1e-7, 4e-7, 64)}
+
+
+def _chain_inputs(args, params, dev, seed):
+    from nipet_b200 import geometry, phantoms
+    lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=seed,
+                                 device=dev)
+    muo = geometry.convert2e7(phantoms.water_mumap(), params['Cnt'])
+    return lm, [np.zeros_like(muo), muo], _norm_components()
+
+
+# our kernels per chain step: histogram 2 (k_hist, k_unpack), prompt gaps 1, norm 2, attenuation
+# 1, randoms 36 (1 + 11 x 3 fixed-point passes + 2), randoms gaps 1, and in Recon: mask 1,
+# (r+s)/(an) 1, 14 sensitivity images, initial image 1, 4 x 14 x 2 sub-iteration kernels,
+# image layout 1
+CHAIN_LAUNCHES = 2 + 1 + 2 + 1 + 36 + 1 + 1 + 1 + 14 + 1 + 4 * 14 * 2 + 1
+
+
+def run_chain(args, ws, rank, dev):
+    import torch
+    from nipet_b200 import geometry, mmr_lmproc, mmrhist, mmrrec
+    from nipet_b200.device import get_geometry
+    params = geometry.get_mmrparams()
+    sp = dict(params, Cnt=dict(params['Cnt'], SPN=11, DEVID=dev.index))
+    lm, mu, comp = _chain_inputs(args, params, dev, rank)
+    lm_host = lm.cpu().numpy()
+    pl = mmr_lmproc.plan(lm_host)
+
+    def step(stream_words):
+        hst = mmrhist.hist_device(stream_words, sp, pl=pl)
+        return mmrrec.osemone({}, mu, hst, sp, recmod=1, itr=4, normcomp=comp)
+
+    # algorithmic bytes of the fused OSEM launch per subset (as the osem workload)
+    geom = get_geometry(params['txLUT'], params['axLUT'], dev)
+    _, per_lor = geom.count_reads(per_lor=True)
+    tab = mmrrec.subset_table(params)
+    bytes_sub = [8 * int(per_lor[tab[i, 1:]].sum()) + int(tab[i, 0]) * NSN11 * (2 + 4)
+                 for i in range(tab.shape[0])]
+    for _ in range(args.warmup):
+        step(lm)
+    torch.cuda.synchronize(dev)
+    clk = Clocks(dev.index) if rank == 0 else None
+    times, ev = [], []
+    for _ in range(args.steps):
+        _barrier(ws, dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        mmrrec.Recon.event_log = ev
+        t0.record()
+        step(lm)
+        t1.record()
+        mmrrec.Recon.event_log = None
+        _barrier(ws, dev)
+        times.append(t0.elapsed_time(t1) / 1e3)
+    clocks = clk.stop() if clk else None
+    t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
+    dur = [a.elapsed_time(b) / 1e3 for a, b, _ in ev]
+    byt = [bytes_sub[i] for _, _, i in ev]
+    achieved = sum(byt) / sum(dur) / 1e9
+    peak, peak_kind = _peaks()
+    # e2e: the words from pinned host memory, the Siemens-layout image back on the host
+    lm_pin = torch.from_numpy(lm_host).pin_memory()
+    step(lm_pin)
+    et = []
+    for _ in range(max(1, args.e2e_steps)):
+        _barrier(ws, dev)
+        t = time.perf_counter()
+        step(lm_pin)
+        torch.cuda.synchronize(dev)
+        et.append(time.perf_counter() - t)
+    te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    res = {'ms_per_step': t_step * 1e3, 'value': ws / t_step,
+           'e2e': {'value': ws / te, 'unit': 'recon/s', 'h2d_bytes_per_step': int(lm_host.nbytes),
+                   'd2h_bytes_per_step': int(127 * 344 * 344 * 4),
+                   'path': 'mmrhist.hist_device(pinned host words) -> mmrrec.osemone -> host image'},
+           'clocks': clocks, 'gpu_launches': CHAIN_LAUNCHES,
+           'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                        'frac': achieved / peak, 'traffic': _traffic('osem_subiteration'),
+                        'kernel': 'k_project<OSEM> fused sub-iteration inside osemone',
+                        'peak_kind': peak_kind, 'bytes_per_launch_avg': float(np.mean(byt)),
+                        'launch_ms_avg': float(np.mean(dur)) * 1e3},
+           'config': {'workload': f'one frame of the list-mode stream ({lm_host.size} words over '
+                                  f'{args.duration} s) through mmrrec.osemone: span-11 histogram, '
+                                  'randoms from the delayed fan sums, norm from seeded synthetic '
+                                  'components, water mu-map attenuation, 14 sensitivity images, '
+                                  '4 x 14 OSEM (recmod 1, no PSF)',
+                      'global_batch': ws, 'parallelism': f'replicas x{ws}',
+                      'l2': 'inputs larger than L2'}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ch = cpu_hist_sample(lm_host, params)
+        co = cpu_osem_sample(params)
+        t_cpu = lm_host.size / ch['value'] + 1.0 / co['value']
+        res['cpu_baseline'] = {'value': 1.0 / t_cpu, 'unit': 'recon/s', 'cores': co['cores'],
+                               'kind': 'port',
+                               'sample': f"histogram: {ch['sample']}; OSEM: {co['sample']} "
+                                         '(randoms, norm and attenuation not timed)'}
+    return res
+
 # ---------------------------------------------------------------------------------------
 # reference arm: NIPET has no CPU path; its algorithm restated as the FP64 oracle on the
 # host cores (bounded samples of the same workload)
@@ -877,6 +992,57 @@ def run_reference(args):
         line.update({'value': v, 'n_gpus': 1, 'ms_per_step': lm.size / v * 1e3,
                      'dtype': 'u32',
                      'config': {'workload': 'hist', 'implementation':
+                                'reference CUDA (oracle/_ref), compiled for sm_100a'},
+                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
+                                      'kind': 'reference', 'sample': sample}})
+    elif use_cuda and args.workload == 'chain':
+        import torch
+        from nipet_b200 import geometry as G
+        from nipet_b200 import mmrhist, mmrrec
+        from oracle import ref
+        dev = torch.device('cuda', 0)
+        lm_d, mu, comp = _chain_inputs(args, params, dev, 0)
+        lm = lm_d.cpu().numpy()
+        del lm_d
+        Cnt = params['Cnt']
+        aw = np.asarray(params['txLUT']['aw2ali'], np.int64)
+        gapfree = lambda x: np.ascontiguousarray(x.reshape(x.shape[0], -1)[:, aw].T)  # noqa: E731
+        mus = G.convert2dev(mu[1] + mu[0], Cnt)
+        tab = mmrrec.subset_table(params)
+        msk = G.get_cylinder(Cnt, rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
+
+        def one(path):
+            h, _ = ref.hist(params, path, span=11)
+            n = int(h['nitag'])
+            buckets = mmrhist._singles(h['bck'].reshape(2, n, 224), Cnt)[2]
+            nsng = ref.norm(params, comp, buckets, span=11)
+            asng = ref.fprj(params, mus, att=1)[0]
+            rsn, _ = ref.randoms(params, h['fan'].reshape(64, 504), span=11)
+            rsng = gapfree(rsn)
+            psng = gapfree(h['psn'].reshape(837, 252, 344))
+            an = asng * nsng
+            sens = np.stack([ref.bprj(params, an[tab[k, 1:]], tab[k, 1:])[0]
+                             for k in range(tab.shape[0])])
+            x = np.ones((320, 320, 127), np.float32)
+            for _ in range(4):
+                ref.osem(params, x, msk, psng, rsng, np.zeros_like(rsng), nsng, asng, tab, sens)
+            return x
+
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, 'lm.bf')
+            lm.astype('<i4').tofile(path)
+            ts = []
+            for _ in range(args.warmup + args.steps):
+                t = time.perf_counter()
+                one(path)
+                ts.append(time.perf_counter() - t)
+        v = 1.0 / float(np.mean(ts[args.warmup:]))
+        sample = (f'one frame per step ({lm.size} words over {args.duration} s) through the '
+                  'reference CUDA build on this GPU: lmproc on the file, norm_from_components, '
+                  'gpu_fprj (attenuation), gpu_randoms, 14 x gpu_bprj (sensitivity), 4 x osem, '
+                  'with the host arrays and gap removal of osemone')
+        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': 1e3 / v, 'dtype': 'f32',
+                     'config': {'workload': 'chain', 'implementation':
                                 'reference CUDA (oracle/_ref), compiled for sm_100a'},
                      'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
                                       'kind': 'reference', 'sample': sample}})
@@ -982,6 +1148,16 @@ def run_reference(args):
             for _ in range(args.warmup + args.steps):
                 c = cpu_osem_sample(params, seconds=6.0)
                 vals.append(dict(c, value=c['value'] * f, unit=unit))
+        elif args.workload == 'chain':
+            from nipet_b200 import phantoms
+            lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
+            for _ in range(args.warmup + args.steps):
+                c = cpu_osem_sample(params, seconds=6.0)
+                h = cpu_hist_sample(lm, params)
+                t = (args.events + 1000 * args.duration) / h['value'] + 1.0 / c['value']
+                vals.append(dict(c, value=1.0 / t, unit=unit,
+                                 sample=f"histogram {h['sample']} scaled to the stream; "
+                                        f"OSEM {c['sample']}"))
         else:
             from nipet_b200 import phantoms
             lm = phantoms.lm_stream(2_000_000, 60, seed=0, params=params)
@@ -1010,7 +1186,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='batch',
-                    choices=['batch', 'osem', 'hist', 'diff', 'dynamic'])
+                    choices=['batch', 'osem', 'hist', 'diff', 'dynamic', 'chain'])
     ap.add_argument('--replicates', type=int, default=50)
     ap.add_argument('--plain-steps', type=int, default=1)
     ap.add_argument('--e2e-steps', type=int, default=1)
@@ -1032,7 +1208,7 @@ def main():
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
     run = {'batch': run_batch, 'osem': run_osem, 'hist': run_hist, 'diff': run_diff,
-           'dynamic': run_dynamic}[args.workload]
+           'dynamic': run_dynamic, 'chain': run_chain}[args.workload]
     res = run(args, ws, rank, dev)
     metric, unit = METRIC[args.workload]
     if rank == 0:

@@ -60,14 +60,7 @@ def hist(datain, txLUT, axLUT, Cnt, t0=0, t1=0, cmass_sig=5, frms=None, use_stor
     pvs_sgtl = np.right_shift(hstout['pvs'], 8).astype(np.float32)
     pvs_crnl = np.bitwise_and(hstout['pvs'], 255).astype(np.float32)
     cmass = Cnt['SO_VXZ'] * ndi.gaussian_filter(hstout['mss'], cmass_sig, mode='mirror')
-    nsr = hstout['bck'][1, :, :] >> 30
-    bck0 = hstout['bck'][0].copy()
-    bck0[nsr > 0] = bck0[nsr > 0] / nsr[nsr > 0]
-    tmsk = np.sum(nsr, axis=1) > 0
-    single_rate = np.copy(bck0[tmsk, :])
-    t = np.arange(nitag)[tmsk]
-    buckets = (np.int32(np.sum(single_rate, axis=0) / single_rate.shape[0])
-               if single_rate.shape[0] else np.zeros(Cnt['NBCKT'], np.int32))
+    single_rate, t, buckets = _singles(hstout['bck'], Cnt)
     if t0 == t1:
         t1 = t0 + nitag
     return {'t0': t0, 't1': t1, 'dur': t1 - t0, 'phc': hstout['phc'], 'dhc': hstout['dhc'],
@@ -75,6 +68,46 @@ def hist(datain, txLUT, axLUT, Cnt, t0=0, t1=0, cmass_sig=5, frms=None, use_stor
             'fansums': hstout['fan'], 'sngl_rate': single_rate, 'tsngl': t,
             'buckets': buckets, 'psino': hstout['psn'].astype(np.uint16),
             'dsino': hstout['dsn'].astype(np.uint16), 'pssr': hstout['ssr']}
+
+
+def _singles(bck, Cnt):
+    """Singles rates per reported second, their seconds and the mean bucket singles
+    (`lm/mmrhist.py:160-172`) from the histogram's `bck` [2, nitag, 224] counters."""
+    bck = np.asarray(bck)
+    nsr = bck[1, :, :] >> 30
+    bck0 = bck[0].copy()
+    bck0[nsr > 0] = bck0[nsr > 0] / nsr[nsr > 0]
+    tmsk = np.sum(nsr, axis=1) > 0
+    single_rate = np.copy(bck0[tmsk, :])
+    t = np.arange(bck.shape[1])[tmsk]
+    buckets = (np.int32(np.sum(single_rate, axis=0) / single_rate.shape[0])
+               if single_rate.shape[0] else np.zeros(Cnt['NBCKT'], np.int32))
+    return single_rate, t, buckets
+
+
+def hist_device(lm, scanner_params, t0=0, t1=0, cmass_sig=5, pl=None):
+    """`hist` of a word stream already in memory (host int32 words or a CUDA tensor), with
+    the same dictionary keys; the sinograms (`psino`, `dsino`, `pssr`), fan sums, head
+    curves and projection views stay on the device as CUDA tensors, the singles and the
+    centre of mass come back to the host.  `pl`, a chunk plan of the stream
+    (`mmr_lmproc.plan`), saves re-planning it."""
+    import torch
+    from . import mmr_lmproc
+    Cnt, txLUT, axLUT = (scanner_params['Cnt'], scanner_params['txLUT'],
+                         scanner_params['axLUT'])
+    r = mmr_lmproc.hist_stream(lm, txLUT, axLUT, dict(Cnt, BTP=0), t0=t0, t1=t1, pl=pl)
+    nitag = int(r['nitag'])
+    single_rate, t, buckets = _singles(r['bck'].cpu().numpy(), Cnt)
+    mss = r['mss'].cpu().numpy()
+    cmass = Cnt['SO_VXZ'] * ndi.gaussian_filter(mss, cmass_sig, mode='mirror')
+    if t0 == t1:
+        t1 = t0 + nitag
+    pvs = r['pvs'].to(torch.int64)
+    return {'t0': t0, 't1': t1, 'dur': t1 - t0, 'phc': r['phc'], 'dhc': r['dhc'],
+            'cmass': cmass, 'pvs_sgtl': (pvs >> 8).to(torch.float32),
+            'pvs_crnl': (pvs & 255).to(torch.float32), 'fansums': r['fan'],
+            'sngl_rate': single_rate, 'tsngl': t, 'buckets': buckets, 'psino': r['psn'],
+            'dsino': r['dsn'], 'pssr': r['ssr']}
 
 
 # ---------------------------------------------------------------------------------------

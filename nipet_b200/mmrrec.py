@@ -159,6 +159,10 @@ class Recon:
     are convolved once and every sub-iteration convolves the image before the forward
     projection and the back projection before the update (`recon.cu:437-497`)."""
 
+    # when a list, every sub-iteration appends (start, stop, subset) CUDA events recorded
+    # around its launches (for timing a reconstruction run inside a larger call)
+    event_log = None
+
     def __init__(self, params: dict, psng, rsng, nsng, asng, ssng=None, device=None,
                  nsub: int = 14, mask_radius: float = 29.0, krnl=None):
         self.device = torch.device(device or 'cuda')
@@ -219,6 +223,17 @@ class Recon:
         return to_col128(ones).reshape(-1)
 
     def subiteration(self, img128: torch.Tensor, i: int, stream=None):
+        log = Recon.event_log
+        if log is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        self._subiteration(img128, i, stream)
+        if log is not None:
+            e1.record()
+            log.append((e0, e1, i))
+
+    def _subiteration(self, img128: torch.Tensor, i: int, stream=None):
         st = stream if stream is not None else stream_ptr(self.device)
         if self.krnl is not None:
             _lib.check(self.lib.nb_osem_subset_psf(
@@ -305,7 +320,7 @@ def decay_quant_factors(hst: dict, Cnt: dict, ncmp: dict, decay_ref_time=None):
         else:
             dcycrr = 1.
         if ncmp.get('qf') is None:
-            log.warning('norm components carry no quantification factor: qf = 1')
+            log.info('norm components carry no quantification factor: qf = 1')
             return dcycrr, 1., 1.
         return dcycrr, ncmp['qf'] / iso['BF'] / float(hst['dur']), ncmp.get('qf_loc', 1.)
     return 1., 1., 1.

@@ -84,3 +84,15 @@ def test_mmrchain_frames_equal_osemone(params, cuda_device, scan):
         rl2 = np.linalg.norm(one.im.astype(np.float64) - o['im'][i]) / np.linalg.norm(one.im)
         assert rl2 <= 1e-6, f'frame {i}: relative L2 {rl2:.3e}'
     assert o['im'][0].sum() > 0 and o['im'][1].sum() > 0
+
+
+def test_hist_device_matches_file_histogram(params, cuda_device, scan):
+    lm = np.fromfile(scan['datain']['lm_bf'], '<i4')
+    a = mmrhist.mmrhist(scan['datain'], params)
+    b = mmrhist.hist_device(lm, params)
+    for k in ('psino', 'dsino', 'pssr', 'phc', 'dhc', 'fansums'):
+        g = b[k].cpu().numpy().astype(np.int64).reshape(-1)
+        assert np.array_equal(np.asarray(a[k]).astype(np.int64).reshape(-1), g), k
+    assert np.array_equal(a['buckets'], b['buckets'])
+    assert (a['t0'], a['t1'], a['dur']) == (b['t0'], b['t1'], b['dur'])
+    assert np.array_equal(a['cmass'], b['cmass'])
