@@ -65,10 +65,7 @@ class BatchRecon:
         tab = subset_table(params, nsub)
         self.nsub, self.nprj = tab.shape[0], int(tab[0, 0])
         self.subs = [torch.from_numpy(tab[i, 1:]).to(dev) for i in range(self.nsub)]
-        msk = geometry.get_cylinder(params['Cnt'], rad=mask_radius, xo=0, yo=0, unival=1,
-                                    gpu_dim=True) > 0.9
-        self.msk128 = (to_col128(torch.from_numpy(msk.astype(np.float32)).to(dev)) > 0.5).to(
-            torch.uint8).reshape(-1)
+        self.msk128 = geometry.cylinder_mask128(params['Cnt'], mask_radius, dev)
         self.sens128 = torch.empty((self.nsub, COL128), device=dev)
         self.graph = None
         self.launches = 0

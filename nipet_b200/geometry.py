@@ -329,23 +329,50 @@ def get_cylinder(Cnt: dict, rad=25, xo=0, yo=0, unival=1, gpu_dim=False) -> np.n
     return imdsk
 
 
-def convert2dev(im: np.ndarray, Cnt: dict) -> np.ndarray:
-    """Siemens (z, 344, 344) -> GPU (320, 320, z) layout (`img/mmrimg.py:48-67`)."""
+def convert2dev(im, Cnt: dict):
+    """Siemens (z, 344, 344) -> GPU (320, 320, z) layout (`img/mmrimg.py:48-67`); a torch
+    tensor is converted on its own device."""
     if im.shape[1] != Cnt['SO_IMY'] or im.shape[2] != Cnt['SO_IMX']:
         raise ValueError('input image array is not of the correct Siemens shape')
     m = (Cnt['SO_IMX'] - Cnt['SZ_IMX']) // 2
     ims = im[:, m:-m, m:-m] if m else im
+    if not isinstance(im, np.ndarray) and hasattr(im, 'permute'):
+        return ims.permute(1, 2, 0).contiguous()
     return np.ascontiguousarray(np.transpose(ims, (1, 2, 0)))
 
 
-def convert2e7(img: np.ndarray, Cnt: dict) -> np.ndarray:
-    """GPU (320, 320, z) -> Siemens (z, 344, 344) layout (`img/mmrimg.py:28-45`)."""
+def convert2e7(img, Cnt: dict):
+    """GPU (320, 320, z) -> Siemens (z, 344, 344) layout (`img/mmrimg.py:28-45`); a torch
+    tensor is converted on its own device (float32 out)."""
     m = (Cnt['SO_IMX'] - Cnt['SZ_IMX']) // 2
+    if not isinstance(img, np.ndarray) and hasattr(img, 'permute'):
+        import torch
+        imo = img.permute(2, 0, 1)
+        out = torch.zeros((imo.shape[0], Cnt['SO_IMY'], Cnt['SO_IMX']), dtype=torch.float32,
+                          device=img.device)
+        out[:, m:m + Cnt['SZ_IMY'], m:m + Cnt['SZ_IMX']] = imo
+        return out
     imo = np.transpose(np.asarray(img), (2, 0, 1))
     nvz = imo.shape[0]
     out = np.zeros((nvz, Cnt['SO_IMY'], Cnt['SO_IMX']), dtype=np.float32)
     out[:, m:m + Cnt['SZ_IMY'], m:m + Cnt['SZ_IMX']] = imo
     return out
+
+
+_MASKS: dict = {}
+
+
+def cylinder_mask128(Cnt: dict, rad: float, device):
+    """The reconstruction mask (`get_cylinder(Cnt, rad, gpu_dim=True) > 0.9`) in the col128
+    layout as uint8 on `device`, built once per (radius, device) and cached."""
+    import torch
+    from .petprj import to_col128
+    key = (float(rad), str(torch.device(device)), int(Cnt['SO_IMX']), int(Cnt['SZ_IMZ']))
+    if key not in _MASKS:
+        msk = get_cylinder(Cnt, rad=rad, xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
+        _MASKS[key] = (to_col128(torch.from_numpy(msk.astype(np.float32)).to(device)) > 0.5).to(
+            torch.uint8).reshape(-1)
+    return _MASKS[key]
 
 
 def mmrinit() -> tuple[dict, dict, dict]:

@@ -179,10 +179,7 @@ class Recon:
         tab = subset_table(params, nsub)
         self.nsub, self.nprj = tab.shape[0], int(tab[0, 0])
         self.subs = [torch.from_numpy(tab[i, 1:]).to(dev) for i in range(self.nsub)]
-        msk = geometry.get_cylinder(params['Cnt'], rad=mask_radius, xo=0, yo=0, unival=1,
-                                    gpu_dim=True) > 0.9
-        self.msk128 = (to_col128(torch.from_numpy(msk.astype(np.float32)).to(dev)) > 0.5).to(
-            torch.uint8).reshape(-1)
+        self.msk128 = geometry.cylinder_mask128(params['Cnt'], mask_radius, dev)
         st = stream_ptr(dev)
         self.rs = torch.empty((NAW, 837), device=dev)
         _lib.check(self.lib.nb_osem_rs(dev_ptr(self.rs), dev_ptr(self.rsng),
@@ -369,7 +366,9 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
         asng = _gapfree(attnsino, txLUT, Cnt, dev, torch.float32)
     else:
         muh, muo = mumaps
-        mus = geo.convert2dev(np.asarray(muo, np.float32) + np.asarray(muh, np.float32), Cnt)
+        as_dev = lambda m: torch.as_tensor(np.asarray(m, np.float32) if not isinstance(  # noqa: E731
+            m, torch.Tensor) else m).to(dev, torch.float32)
+        mus = geo.convert2dev(as_dev(muo) + as_dev(muh), Cnt)
         asng = attenuation_sino(mus, scanner_params, dev)
     # randoms
     if randsino is not None:
@@ -390,8 +389,7 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
             break
     rec.geom.check()
     dcycrr, qf, qf_loc = decay_quant_factors(hst, Cnt, ncmp, decay_ref_time)
-    x = rec.image(img).cpu().numpy() * np.float32(dcycrr * qf * qf_loc)
-    im = geo.convert2e7(x, Cnt)
+    im = geo.convert2e7(rec.image(img) * np.float32(dcycrr * qf * qf_loc), Cnt).cpu().numpy()
     opth = outpath if outpath is not None else os.path.join(datain.get('corepath', ''),
                                                             'reconstructed')
     if fout is None:
