@@ -122,3 +122,14 @@ def test_osem_without_prompts_gives_a_zero_image(params, cuda_device, psf):
                 tab, sens, msk, mmrrec.psf_config(psf, params['Cnt']), params['txLUT'],
                 params['axLUT'], params['Cnt'])
     assert not x[msk].any()
+
+
+def test_cylinder_mask_is_cached(params, cuda_device):
+    import torch
+    m1 = geometry.cylinder_mask128(params['Cnt'], 29.0, cuda_device)
+    m2 = geometry.cylinder_mask128(params['Cnt'], 29.0, cuda_device)
+    assert m1 is m2 and m1.dtype == torch.uint8 and m1.numel() == petprj.COL128
+    ref = geometry.get_cylinder(params['Cnt'], rad=29.0, xo=0, yo=0, unival=1,
+                                gpu_dim=True) > 0.9
+    back = petprj.from_col128(m1.reshape(1, -1).to(torch.float32))[0].cpu().numpy() > 0.5
+    assert np.array_equal(back, ref)

@@ -80,3 +80,32 @@ def test_osemone_and_mmrchain_argument_checks(params):
         pipe.mmrchain({}, params, store_img=True)
     with pytest.raises(NotImplementedError, match='NIfTI'):
         pipe._mu('mumap.nii.gz')
+
+
+def test_singles_from_bucket_counters(params):
+    from nipet_b200 import mmrhist
+    nitag = 5
+    bck = np.zeros((2, nitag, 224), np.uint32)
+    # seconds 1 and 3 report singles: counts 800 and 1200 in bucket 7, reported twice in
+    # second 3 (the report count sits in the top bits of the second array)
+    bck[0, 1, 7], bck[1, 1, 7] = 800, 1 << 30
+    bck[0, 3, 7], bck[1, 3, 7] = 2400, 2 << 30
+    rate, t, buckets = mmrhist._singles(bck, params['Cnt'])
+    assert list(t) == [1, 3]
+    assert rate.shape == (2, 224) and rate[0, 7] == 800 and rate[1, 7] == 1200
+    assert buckets.dtype == np.int32 and buckets[7] == 1000 and buckets.sum() == 1000
+    _, t0, b0 = mmrhist._singles(np.zeros((2, nitag, 224), np.uint32), params['Cnt'])
+    assert t0.size == 0 and not b0.any()
+
+
+def test_layout_conversions_on_tensors_match_numpy(params):
+    import torch
+    from nipet_b200 import geometry
+    rng = np.random.default_rng(0)
+    e7 = rng.random((127, 344, 344)).astype(np.float32)
+    dev = geometry.convert2dev(e7, params['Cnt'])
+    dev_t = geometry.convert2dev(torch.from_numpy(e7), params['Cnt'])
+    assert np.array_equal(dev, dev_t.numpy())
+    back = geometry.convert2e7(dev, params['Cnt'])
+    back_t = geometry.convert2e7(torch.from_numpy(dev), params['Cnt'])
+    assert np.array_equal(back, back_t.numpy())
