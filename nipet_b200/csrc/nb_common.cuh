@@ -111,6 +111,16 @@ static __device__ __forceinline__ void nb_bulk_reduce_add_f32(float *dst_gmem,
                : "memory");
 }
 
+// shared -> global bulk reduction (element-wise uint32 add performed at L2, wrapping)
+static __device__ __forceinline__ void nb_bulk_reduce_add_u32(uint32_t *dst_gmem,
+                                                              const uint32_t *src_smem,
+                                                              uint32_t bytes) {
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u32 [%0], [%1], %2;" ::"l"(
+                   dst_gmem),
+               "r"(nb_smem_u32(src_smem)), "r"(bytes)
+               : "memory");
+}
+
 static __device__ __forceinline__ void nb_bulk_commit() {
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }

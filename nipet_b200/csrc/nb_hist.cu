@@ -27,8 +27,10 @@
 // replicates side by side, so one event's replicate updates share one or two L2
 // sectors), then packs it into the caller's sinograms (prompts + 65536 x delayeds, the
 // reference's uint32 sum) and sums the SSRB counters from the prompts (every output
-// sinogram lies in one SSRB sinogram), so the SSRB counters take no atomics.  A single
-// histogram, and nb_hist_static (which may not allocate), count both directly.
+// sinogram lies in one SSRB sinogram), so the SSRB counters take no atomics; an event's
+// replicate weights are staged in shared memory and added to its bin's replicate block by
+// one bulk reduce-add (cp.reduce.async.bulk .add.u32) instead of one atomic per replicate.
+// A single histogram, and nb_hist_static (which may not allocate), count both directly.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -65,9 +67,11 @@ struct HistArgs {
   size_t nbins, sne;
   uint32_t *psino, *ssrb, *phc, *dhc, *pvs, *fan, *bck;
   int32_t *zR, *zM;
-  int unp;                  // 1: psino is an unpacked scratch [bin][2][nrep] (prompts,
+  int unp;                  // 1: psino is an unpacked scratch [bin][2][rblk] (prompts,
                             // delayeds) and SSRB is derived afterwards; 0: packed
                             // [nrep][bin] with SSRB counted here
+  int rblk;                 // unpacked scratch: replicate block length (nrep rounded up to 4)
+  int bulk;                 // unpacked scratch: one bulk reduce-add per event for all replicates
   unsigned *next_slice;     // work counter, 0 at launch
 };
 
@@ -197,13 +201,17 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   const int lane = threadIdx.x & 31;
   uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * a.nrep;
   for (int r = lane; r < 3 * a.nrep; r += 32) acc[r] = 0;
+  // bulk mode: two staging rows of rblk weights per thread, after the accumulators (both
+  // offsets are multiples of 16 bytes, as the bulk copy needs)
+  uint32_t *const stg = s_acc + (size_t)8 * 3 * a.nrep + (size_t)threadIdx.x * 2 * a.rblk;
+  int par = 0;
   __syncthreads();
 
   const int nslices = a.nchnk * NB_TOTHRDS;
   // replicate / bin strides of the two large counter arrays
   // replicate / bin strides of the sinogram counters, the delayed slot offset and shift
-  const size_t pstr_r = a.unp ? 1 : a.nbins, pstr_b = a.unp ? 2 * (size_t)a.nrep : 1;
-  const size_t doff = a.unp ? (size_t)a.nrep : 0;
+  const size_t pstr_r = a.unp ? 1 : a.nbins, pstr_b = a.unp ? 2 * (size_t)a.rblk : 1;
+  const size_t doff = a.unp ? (size_t)a.rblk : 0;
   const int dshift = a.unp ? 0 : 16;
   const size_t sstr_r = (size_t)NB_SEG0 * NB_NSBINANG;
   for (;;) {
@@ -333,6 +341,10 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         uint32_t *const ss0 = a.ssrb + sbin;
         uint32_t blk[4] = {0u, 0u, 0u, 0u};
         int qblk = -1;
+        uint32_t *const row = stg + par * a.rblk;
+        // the row's previous bulk add (two steps back) must have read it
+        if (a.bulk) nb_bulk_wait_read<1>();
+        bool any = false;
         for (int r = 0; r < a.nrep; r++) {
           const int rep = a.rep0 + r;
           uint32_t N = 1;
@@ -362,8 +374,12 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
             N = k;
           }
           const bool ok = okb && N > 0 && N < 32;
+          if (a.bulk) {
+            row[r] = ok ? N : 0u;
+            any |= ok;
+          }
           if (ok) {
-            atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
+            if (!a.bulk) atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
             if (e.prompt) {
               if (!a.unp) atomicAdd(ss0 + (size_t)r * sstr_r, N);
               if (pv) atomicAdd(a.pvs + (size_t)r * a.sne + pvo, N << ((e.an == 126) * 8));
@@ -377,6 +393,16 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           const uint32_t nn = ok ? N : 0u;
           second_sums(a, acc, r, uni, ok, itag, e.prompt ? nn : 0u, e.prompt ? 0u : nn,
                       (ok && e.prompt) ? (uint32_t)e.sis : 0u, lane);
+        }
+        if (a.bulk) {
+          // all replicates of the event in one L2 reduction of the bin's replicate block
+          for (int r = a.nrep; r < a.rblk; r++) row[r] = 0u;
+          if (any) {
+            nb_fence_proxy_async_smem();
+            nb_bulk_reduce_add_u32(ps0, row, 4u * (uint32_t)a.rblk);
+          }
+          nb_bulk_commit();  // one group per step, empty or not: groups alternate rows
+          par ^= 1;
         }
         continue;
       }
@@ -427,17 +453,18 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
     }
     flush_seconds(a, acc, acc_sec, lane);
   }
+  if (a.bulk) nb_bulk_wait_all<0>();
 }
 
-// Unpacked scratch [bin][2][nrep] (prompts, delayeds) added into the caller's packed
+// Unpacked scratch [bin][2][rblk] (prompts, delayeds) added into the caller's packed
 // [nrep][bin] counters: prompts + 65536 x delayeds, the reference's packed uint32 sum
 // (hst.cu:167,192), wrap-around included.
 __global__ void k_pack_add(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
-                           size_t nbins, int nrep) {
+                           size_t nbins, int nrep, int rblk) {
   for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < nbins;
        b += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t *q = src + b * 2 * nrep;
-    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += q[r] + (q[nrep + r] << 16);
+    const uint32_t *q = src + b * 2 * rblk;
+    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += q[r] + (q[rblk + r] << 16);
   }
 }
 
@@ -446,7 +473,7 @@ __global__ void k_pack_add(uint32_t *__restrict__ dst, const uint32_t *__restric
 // of the sinograms listed in src[off[k] .. off[k+1]).
 __global__ void k_ssrb_derive(uint32_t *__restrict__ ssrb, const uint32_t *__restrict__ src,
                               const int *__restrict__ off, const int16_t *__restrict__ lst,
-                              int nrep) {
+                              int nrep, int rblk) {
   const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nss;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -455,7 +482,7 @@ __global__ void k_ssrb_derive(uint32_t *__restrict__ ssrb, const uint32_t *__res
     for (int r = 0; r < nrep; r++) {
       uint32_t acc = 0;
       for (int j = j0; j < j1; j++)
-        acc += src[((size_t)lst[j] * NB_NSBINANG + aw) * 2 * nrep + r];
+        acc += src[((size_t)lst[j] * NB_NSBINANG + aw) * 2 * rblk + r];
       ssrb[(size_t)r * nss + i] += acc;
     }
   }
@@ -601,11 +628,13 @@ static cudaError_t launch_hist(HistArgs &a, unsigned *ctr, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   a.next_slice = ctr;
-  const size_t dyn = (size_t)8 * 3 * a.nrep * sizeof(uint32_t);
+  const size_t dyn = (size_t)8 * 3 * a.nrep * sizeof(uint32_t) +
+                     (a.bulk ? (size_t)256 * 2 * a.rblk * sizeof(uint32_t) : 0);
   int dev = 0, nsm = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (dyn > 48 * 1024) {
+  // static plus dynamic shared memory above 48 KB needs the kernel's opt-in
+  if (dyn + sizeof(HistLUT) + 32 * sizeof(uint64_t) > 48 * 1024) {
     e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
   }
@@ -739,12 +768,15 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   // from the prompts instead of counted per event.  One histogram counts both directly
   // (an unpacked scratch would double its L2 footprint for less than it saves).
   uint32_t *scr = nullptr;
-  const size_t scr_bytes = sizeof(uint32_t) * a.nbins * 2 * (size_t)nrep;
+  const int rblk = (nrep + 3) & ~3;
+  const size_t scr_bytes = sizeof(uint32_t) * a.nbins * 2 * (size_t)rblk;
   if (e == cudaSuccess && nrep > 1) {
     e = cudaMallocFromPoolAsync((void **)&scr, scr_bytes, pool, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(scr, 0, scr_bytes, s);
     if (e == cudaSuccess) {
       a.unp = 1;
+      a.rblk = rblk;
+      a.bulk = 1;
       a.psino = scr;
     }
   }
@@ -753,8 +785,8 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    k_pack_add<<<nsm * 8, 256, 0, s>>>(psino, scr, a.nbins, nrep);
-    k_ssrb_derive<<<nsm * 8, 256, 0, s>>>(ssrb, scr, d_soff, d_slst, nrep);
+    k_pack_add<<<nsm * 8, 256, 0, s>>>(psino, scr, a.nbins, nrep, rblk);
+    k_ssrb_derive<<<nsm * 8, 256, 0, s>>>(ssrb, scr, d_soff, d_slst, nrep, rblk);
     e = cudaGetLastError();
   }
   // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go

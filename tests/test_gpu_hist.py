@@ -65,6 +65,20 @@ def test_hist_bootstrap_replicates(params, stream, cuda_device, btp):
     assert p0 != p1
 
 
+@pytest.mark.parametrize('span', [11, 1])
+def test_hist_ten_replicates(params, stream, cuda_device, span):
+    """Ten Poisson replicates in one launch (the bootstrap configuration; its per-thread
+    staging needs more than 48 KB of shared memory per block), first and last replicate
+    checked against the oracle."""
+    Cnt = dict(params['Cnt'], SPN=span, BTP=2, BTPRT=1.0)
+    got = mmr_lmproc.hist_stream(stream, params['txLUT'], params['axLUT'], Cnt, nrep=10,
+                                 rep0=2, seed=99)
+    for r in (0, 9):
+        ref = O.hist(stream, params, span=span, btp=2, btprt=1.0, seed=99, rep=2 + r)
+        _check({k: (v[r] if isinstance(v, torch.Tensor) and v.dim() > 0 and k != 'plan' else v)
+                for k, v in got.items()}, ref)
+
+
 def test_hist_sparse_tags_and_chunks(params, cuda_device):
     """Tags every 50 ms with many events between them: thread slices without a time tag
     (the reference then attributes them to second `nitag`, i.e. drops them), and a stream
