@@ -79,14 +79,15 @@ def _traffic(name):
 class Clocks:
     """nvidia-smi sampler for the timed region."""
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=200):
         self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
         q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
         try:
             self.p = subprocess.Popen(['nvidia-smi', f'--id={index}', f'--query-gpu={q}',
-                                       '--format=csv,noheader,nounits', '-lms', '200'],
+                                       '--format=csv,noheader,nounits', '-lms',
+                                       str(period_ms)],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -866,7 +867,9 @@ def run_chain(args, ws, rank, dev):
     for _ in range(args.warmup):
         step(lm)
     torch.cuda.synchronize(dev)
-    clk = Clocks(dev.index) if rank == 0 else None
+    # a launch-bound step: sample once a second, since each query of the driver competes
+    # with the step's ~170 launches
+    clk = Clocks(dev.index, period_ms=1000) if rank == 0 else None
     times, ev = [], []
     for _ in range(args.steps):
         _barrier(ws, dev)
