@@ -261,6 +261,14 @@ int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const int64_t *ata
 int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t *dsn,
                    unsigned long long *psum, unsigned long long *dsum, void *stream);
 
+/* nb_hist_trim has no counterpart in the reference.  nb_hist takes its stream-ordered
+ * scratch (tables, and for bootstrap replicates the unpacked counters: 8 x nbins x rblk
+ * bytes, rblk = nrep rounded up to 4 -- about 7 GB for 10 span-11 replicates) from a
+ * memory pool of its own per device that keeps freed memory for the next call.  This
+ * returns the current device's unused pool memory to the system (cudaMemPoolTrimTo 0);
+ * memory of calls still in flight on a stream stays until they finish. */
+int nb_hist_trim(void);
+
 #ifdef __cplusplus
 }
 #endif

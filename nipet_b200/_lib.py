@@ -65,6 +65,7 @@ SIGNATURES = {
                         P, P, P, P, P, P, P, P, P, P, P, P, P, P], I),
     'nb_hist_unpack':([P, C.c_size_t, P, P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                         P], I),
+    'nb_hist_trim': ([], I),
 }
 
 _lib = None

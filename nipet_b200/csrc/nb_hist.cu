@@ -622,6 +622,13 @@ static cudaError_t hist_pool(cudaMemPool_t *out) {
   return cudaSuccess;
 }
 
+extern "C" int nb_hist_trim(void) {
+  cudaMemPool_t pool = nullptr;
+  NB_CUDA(hist_pool(&pool));
+  NB_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return NB_OK;
+}
+
 // Launch the persistent histogram kernel: as many 256-thread blocks as fit on the device at
 // once, each warp pulling thread slices from the counter `ctr` (zeroed here).
 static cudaError_t launch_hist(HistArgs &a, unsigned *ctr, cudaStream_t s) {

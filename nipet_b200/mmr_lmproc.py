@@ -161,3 +161,9 @@ def hist(dicout: dict, path: str, t0: int, t1: int, txLUT: dict, axLUT: dict, Cn
         dst = dicout[k]
         src = r[k].cpu().numpy()
         np.copyto(dst.reshape(-1)[:src.size], src.reshape(-1).astype(dst.dtype, copy=False))
+
+
+def trim():
+    """Return the histogrammer's unused scratch memory on the current device
+    (`nb_hist_trim`): bootstrap calls keep their replicate scratch for the next call."""
+    _lib.check(_lib.load().nb_hist_trim())

@@ -110,3 +110,17 @@ def test_lminfo_and_hist_file_api(params, stream, cuda_device, tmp_path):
     ref = O.hist(stream, params, span=11)
     for k in KEYS:
         assert np.array_equal(d[k].reshape(-1), np.asarray(ref[k]).reshape(-1)), k
+
+
+def test_hist_trim_releases_the_replicate_scratch(params, stream, cuda_device):
+    """After a replicate launch the histogrammer's pool keeps its scratch; nb_hist_trim
+    returns it, and later calls allocate again and give the same histograms."""
+    Cnt = dict(params['Cnt'], SPN=11, BTP=2, BTPRT=1.0)
+    a = mmr_lmproc.hist_stream(stream, params['txLUT'], params['axLUT'], Cnt, nrep=4, seed=3)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    mmr_lmproc.trim()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 - free0 >= 72557856 * 8 * 4 * 0.9   # the span-11 scratch of 4 replicates
+    b = mmr_lmproc.hist_stream(stream, params['txLUT'], params['axLUT'], Cnt, nrep=4, seed=3)
+    assert torch.equal(a['psino'], b['psino']) and torch.equal(a['ssr'], b['ssr'])
