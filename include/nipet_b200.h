@@ -123,6 +123,16 @@ int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens1
                    const uint8_t *msk128, const uint16_t *psng, const float *rs,
                    const int32_t *subs, int nprj, void *stream);
 
+/* nb_osem_subset_span1: one span-1 OSEM sub-iteration of one image, the reference's
+ * osem() with Cnt.SPN == 1 (recon.cu:318-497): psng [68516][4084] uint16 prompts, rs
+ * [68516][4084] float from nb_osem_rs, the other arguments as nb_osem_subset; krnl
+ * (host [3][17], NULL for none) applies the resolution kernel as nb_osem_subset_psf, with
+ * work128 two col128 images of scratch. */
+int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128, const float *sens128,
+                         const uint8_t *msk128, const uint16_t *psng, const float *rs,
+                         const int32_t *subs, int nprj, const float *krnl, float *work128,
+                         void *stream);
+
 /* Resolution modelling (recon.cu:49-216, the PSF of petprj.osem when krnl[0][0] >= 0).
  * nb_psf_col128: the reference's separable convolution of one col128 image -- along z
  *   with krnl row 0, then x with row 1, then y with row 2 (the row order psf_config,

@@ -736,6 +736,57 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
   return NB_OK;
 }
 
+extern "C" int nb_psf_col128(float *dst128, const float *src128, const float *krnl,
+                             float *tmp128, void *stream);
+
+// One span-1 OSEM sub-iteration of one image (the reference's osem() with Cnt.SPN == 1,
+// recon.cu:318-497): the batched kernel with one image per walk, whose layout is the col128
+// image itself, then the update; with a PSF kernel (krnl, [3][17], may be NULL) the forward
+// projection sees the convolved image and the back projection is convolved before the
+// update, as nb_osem_subset_psf does at span 11.  work128: two col128 images (PSF only).
+extern "C" int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128,
+                                    const float *sens128, const uint8_t *msk128,
+                                    const uint16_t *psng, const float *rs, const int32_t *subs,
+                                    int nprj, const float *krnl, float *work128, void *stream) {
+  NB_REQUIRE(g != nullptr, "nb_osem_subset_span1: NULL geometry handle");
+  NB_REQUIRE(img128 && bimg128 && sens128 && msk128 && psng && rs && subs,
+             "nb_osem_subset_span1: NULL argument");
+  NB_REQUIRE(!krnl || work128, "nb_osem_subset_span1: the PSF needs work128");
+  NB_REQUIRE(nprj > 0 && nprj <= g->naw, "nb_osem_subset_span1: bad subset size");
+  NB_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  float *rm = krnl ? work128 : nullptr, *tmp = krnl ? work128 + NB_IMG_COL128 : nullptr;
+  if (krnl) {
+    const int st = nb_psf_col128(rm, img128, krnl, tmp, stream);
+    if (st) return st;
+  }
+  NB_CUDA(cudaMemsetAsync(bimg128, 0, sizeof(float) * NB_IMG_COL128, s));
+  float *one = nullptr;  // the randoms factor of the single image
+  NB_CUDA(cudaMallocAsync((void **)&one, sizeof(float), s));
+  const float h_one = 1.f;  // a pageable-source async copy is staged before it returns
+  cudaError_t e = cudaMemcpyAsync(one, &h_one, sizeof(float), cudaMemcpyHostToDevice, s);
+  int st = NB_OK;
+  if (e == cudaSuccess) {
+    nbb::BatchArgs a{};
+    batch_geometry(g, a, 1, 1, 1, subs, nprj);
+    a.img = krnl ? rm : img128;
+    a.bimg = bimg128;
+    a.psng = psng;
+    a.rs = rs;
+    a.rscale = one;
+    st = launch_batch<1, 64, NB_NSN1, 1024, 4>(g, a, s);
+    if (!st && krnl) st = nb_psf_col128(rm, bimg128, krnl, tmp, stream);
+    if (!st) {
+      k_update_batch<1><<<dim3(g->nsm * 4, 1), 256, 0, s>>>(img128, krnl ? rm : bimg128,
+                                                            sens128, msk128, 1);
+      e = cudaGetLastError();
+    }
+  }
+  cudaFreeAsync(one, s);
+  if (e != cudaSuccess) return nb_cuda_fail(e, "nb_osem_subset_span1", __FILE__, __LINE__);
+  return st;
+}
+
 extern "C" int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep, int bs,
                              int span, const int32_t *subs, int nprj, void *stream) {
   NB_REQUIRE(g != nullptr, "nb_fprj_batch: NULL geometry handle");

@@ -134,7 +134,8 @@ def from_col128(im128: torch.Tensor, nimg: int = 1) -> torch.Tensor:
 
 def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axLUT, cnst):
     """One OSEM iteration over all subsets, updating `img` in place, as `petprj.osem`
-    (`prj_module.cu:613-839`, `recon.cu:318-521`).
+    (`prj_module.cu:613-839`, `recon.cu:318-521`), for span-11 or span-1 sinograms
+    (`cnst['SPN']`; span 1 runs the batched kernel with one image per walk).
 
     `subs` is `[Nsub, 1+Nprj]` with `subs[i,0] = Nprj`; `sensimg` is `[Nsub,320,320,127]`;
     `krnl` `[3, 17]` is the resolution-modelling kernel (rows z, x, y as `psf_config`
@@ -143,15 +144,16 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     projection and the back projection before the update, as the reference does
     (`recon.cu:437-497`)."""
     dev = device_of(cnst)
-    if int(cnst['SPN']) != 11:
-        raise NotImplementedError('nipet_b200.petprj.osem runs span-11 data')
+    span = int(cnst['SPN'])
+    if span not in (1, 11):
+        raise ValueError(f'unrecognised span {span}')
     k = np.ascontiguousarray(np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor) else krnl,
                                         dtype=np.float32).reshape(-1))
     use_psf = k.size > 0 and k[0] >= 0
     if use_psf and k.size != 3 * 17:
         raise ValueError('krnl must have shape (3, 17)')
     g = get_geometry(txLUT, axLUT, dev)
-    nsn = 837
+    nsn = 837 if span == 11 else 4084
     lib = _lib.load()
     st = stream_ptr(dev)
     subs_np = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs)
@@ -185,7 +187,13 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     for i in range(nsub):
         nprj = int(subs_np[i, 0])
         d_sub = to_device(subs_np[i, 1:1 + nprj].astype(np.int32), np.int32, dev)
-        if use_psf:
+        if span == 1:
+            _lib.check(lib.nb_osem_subset_span1(g.handle, dev_ptr(img128), dev_ptr(bimg128),
+                                                dev_ptr(sens128[i]), dev_ptr(msk128),
+                                                dev_ptr(d_psng), dev_ptr(rs), dev_ptr(d_sub),
+                                                nprj, kp if use_psf else None,
+                                                dev_ptr(work) if use_psf else None, st))
+        elif use_psf:
             _lib.check(lib.nb_osem_subset_psf(g.handle, dev_ptr(img128), dev_ptr(bimg128),
                                               dev_ptr(sens128[i]), dev_ptr(msk128),
                                               dev_ptr(d_psng), dev_ptr(rs), dev_ptr(d_sub),
