@@ -154,17 +154,22 @@ def synthetic_scan(params: dict, device, seed: int = 0, counts: float = 3e7,
 
 
 class Recon:
-    """Device-resident OSEM (span 11) for one scan; `krnl` [3, 17] (as `psf_config` builds
-    it, `krnl[0, 0] < 0` = off) switches on resolution modelling: the sensitivity images
-    are convolved once and every sub-iteration convolves the image before the forward
-    projection and the back projection before the update (`recon.cu:437-497`)."""
+    """Device-resident OSEM for one scan (span 11, or span 1 with `span=1`); `krnl`
+    [3, 17] (as `psf_config` builds it, `krnl[0, 0] < 0` = off) switches on resolution
+    modelling: the sensitivity images are convolved once and every sub-iteration convolves
+    the image before the forward projection and the back projection before the update
+    (`recon.cu:437-497`)."""
 
     # when a list, every sub-iteration appends (start, stop, subset) CUDA events recorded
     # around its launches (for timing a reconstruction run inside a larger call)
     event_log = None
 
     def __init__(self, params: dict, psng, rsng, nsng, asng, ssng=None, device=None,
-                 nsub: int = 14, mask_radius: float = 29.0, krnl=None):
+                 nsub: int = 14, mask_radius: float = 29.0, krnl=None, span: int = 11):
+        if span not in (1, 11):
+            raise ValueError(f'unrecognised span {span}')
+        self.span = int(span)
+        self.nsn = 837 if self.span == 11 else 4084
         self.device = torch.device(device or 'cuda')
         self.params = params
         self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
@@ -181,10 +186,15 @@ class Recon:
         self.subs = [torch.from_numpy(tab[i, 1:]).to(dev) for i in range(self.nsub)]
         self.msk128 = geometry.cylinder_mask128(params['Cnt'], mask_radius, dev)
         st = stream_ptr(dev)
-        self.rs = torch.empty((NAW, 837), device=dev)
+        for a, nm in ((self.psng, 'psng'), (self.rsng, 'rsng'), (self.nsng, 'nsng'),
+                      (self.asng, 'asng')):
+            if tuple(a.shape) != (NAW, self.nsn):
+                raise ValueError(f'{nm} must have shape {(NAW, self.nsn)} at span {self.span}')
+        self.rs = torch.empty((NAW, self.nsn), device=dev)
         _lib.check(self.lib.nb_osem_rs(dev_ptr(self.rs), dev_ptr(self.rsng),
                                        dev_ptr(self.ssng) if self.ssng is not None else None,
-                                       dev_ptr(self.asng), dev_ptr(self.nsng), NAW * 837, st))
+                                       dev_ptr(self.asng), dev_ptr(self.nsng), NAW * self.nsn,
+                                       st))
         self.an = (self.asng * self.nsng).contiguous()
         self.sens128 = torch.empty((self.nsub, COL128), device=dev)
         self.bimg128 = torch.empty(COL128, device=dev)
@@ -205,7 +215,7 @@ class Recon:
         for i in range(self.nsub):
             _lib.check(self.lib.nb_sens_col128(self.geom.handle, dev_ptr(self.sens128[i]),
                                                dev_ptr(self.an), dev_ptr(self.subs[i]),
-                                               self.nprj, 11, st))
+                                               self.nprj, self.span, st))
             self.launches += 1
             if self.krnl is not None:
                 _lib.check(self.lib.nb_psf_col128(dev_ptr(self.sens128[i]),
@@ -232,6 +242,15 @@ class Recon:
 
     def _subiteration(self, img128: torch.Tensor, i: int, stream=None):
         st = stream if stream is not None else stream_ptr(self.device)
+        if self.span == 1:
+            _lib.check(self.lib.nb_osem_subset_span1(
+                self.geom.handle, dev_ptr(img128), dev_ptr(self.bimg128),
+                dev_ptr(self.sens128[i]), dev_ptr(self.msk128), dev_ptr(self.psng),
+                dev_ptr(self.rs), dev_ptr(self.subs[i]), self.nprj,
+                self.krnl.ctypes.data if self.krnl is not None else None,
+                dev_ptr(self.work) if self.krnl is not None else None, st))
+            self.launches += 2 if self.krnl is None else 8
+            return
         if self.krnl is not None:
             _lib.check(self.lib.nb_osem_subset_psf(
                 self.geom.handle, dev_ptr(img128), dev_ptr(self.bimg128),
@@ -293,14 +312,15 @@ def _gapfree(x, txLUT, Cnt, dev, dtype):
     return t.to(dtype).contiguous()
 
 
-def attenuation_sino(mus, params: dict, device) -> torch.Tensor:
-    """Attenuation factors exp(-integral of mu) [68516, 837] on the device for a GPU-layout
-    (320, 320, 127) mu-map in 1/cm (`petprj.fprj(..., att=1)` over all LORs)."""
+def attenuation_sino(mus, params: dict, device, span: int = 11) -> torch.Tensor:
+    """Attenuation factors exp(-integral of mu) [68516, nsinos] (span 11: 837, span 1:
+    4084) on the device for a GPU-layout (320, 320, 127) mu-map in 1/cm
+    (`petprj.fprj(..., att=1)` over all LORs)."""
     geom = get_geometry(params['txLUT'], params['axLUT'], device)
     mu = (mus if isinstance(mus, torch.Tensor) else torch.from_numpy(
         np.ascontiguousarray(mus, np.float32))).to(device, torch.float32).contiguous()
-    asng = torch.empty((NAW, 837), device=device)
-    _lib.check(_lib.load().nb_fprj(geom.handle, dev_ptr(asng), dev_ptr(mu), None, NAW, 11, 1,
+    asng = torch.empty((NAW, 837 if span == 11 else 4084), device=device)
+    _lib.check(_lib.load().nb_fprj(geom.handle, dev_ptr(asng), dev_ptr(mu), None, NAW, span, 1,
                                    stream_ptr(device)))
     return asng
 
@@ -344,8 +364,10 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
     from scipy import ndimage as ndi
     Cnt, txLUT, axLUT = (scanner_params['Cnt'], scanner_params['txLUT'],
                          scanner_params['axLUT'])
-    if int(Cnt['SPN']) != 11:
-        raise NotImplementedError('osemone reconstructs span-11 data (as petprj.osem)')
+    span = int(Cnt['SPN'])
+    if span not in (1, 11):
+        raise ValueError(f'unrecognised span {span}')
+    nsn = 837 if span == 11 else 4084
     if recmod >= 3:
         raise NotImplementedError('scatter estimation (sct/) is not provided: use recmod=2 '
                                   'with sctsino, or recmod 0/1')
@@ -361,7 +383,7 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
     nsng = mmrnorm.norm_sino(ncmp, hst['buckets'], axLUT, txLUT, Cnt)
     # attenuation factors
     if recmod == 0:
-        asng = torch.ones((NAW, 837), device=dev)
+        asng = torch.ones((NAW, nsn), device=dev)
     elif attnsino is not None:
         asng = _gapfree(attnsino, txLUT, Cnt, dev, torch.float32)
     else:
@@ -369,7 +391,7 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
         as_dev = lambda m: torch.as_tensor(np.asarray(m, np.float32) if not isinstance(  # noqa: E731
             m, torch.Tensor) else m).to(dev, torch.float32)
         mus = geo.convert2dev(as_dev(muo) + as_dev(muh), Cnt)
-        asng = attenuation_sino(mus, scanner_params, dev)
+        asng = attenuation_sino(mus, scanner_params, dev, span)
     # randoms
     if randsino is not None:
         rsng = _gapfree(randsino, txLUT, Cnt, dev, torch.float32)
@@ -378,7 +400,7 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
         rsng = _gapfree(rsn, txLUT, Cnt, dev, torch.float32)
     ssng = _gapfree(sctsino, txLUT, Cnt, dev, torch.float32) if recmod == 2 else None
     rec = Recon(scanner_params, psng, rsng, nsng, asng, ssng, device=dev,
-                mask_radius=mask_radius, krnl=psf_config(psf, Cnt))
+                mask_radius=mask_radius, krnl=psf_config(psf, Cnt), span=span)
     rec.sensitivity()
     img = rec.init_image()
     for k in range(itr):

@@ -93,7 +93,7 @@ def mmrchain(datain, scanner_params, outpath=None, fout=None, frames=None, mu_h=
     if recmod > 0:
         from .device import device_of
         mus = geometry.convert2dev(muo + muh, Cnt)
-        attn = mmrrec.attenuation_sino(mus, scanner_params, device_of(Cnt))
+        attn = mmrrec.attenuation_sino(mus, scanner_params, device_of(Cnt), int(Cnt['SPN']))
     output = {'recmod': recmod, 'frames': t_frms, '#frames': nfrm}
     dynim = np.zeros((nfrm, Cnt['SO_IMZ'], Cnt['SO_IMY'], Cnt['SO_IMX']), np.float32)
     hsts = {}

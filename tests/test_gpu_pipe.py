@@ -96,3 +96,33 @@ def test_hist_device_matches_file_histogram(params, cuda_device, scan):
     assert np.array_equal(a['buckets'], b['buckets'])
     assert (a['t0'], a['t1'], a['dur']) == (b['t0'], b['t1'], b['dur'])
     assert np.array_equal(a['cmass'], b['cmass'])
+
+
+@pytest.mark.skipif(not ref.available(), reason='reference CUDA build (oracle/_ref) not present')
+def test_osemone_span1_matches_reference_chain(params, cuda_device, scan):
+    """osemone on span-1 data (the reference's osemone with Cnt.SPN == 1): histogram,
+    randoms, norm (with the span-1 axial factors), attenuation, sensitivity and OSEM all at
+    span 1, against the same chain from the reference's routines."""
+    comp, _ = _components(7)
+    sp1 = dict(params, Cnt=dict(params['Cnt'], SPN=1))
+    hst = mmrhist.mmrhist(scan['datain'], sp1)
+    out = mmrrec.osemone(scan['datain'], scan['mu'], hst, sp1, recmod=1, itr=1, normcomp=comp)
+    Cnt = params['Cnt']
+    aw = np.asarray(params['txLUT']['aw2ali'], np.int64)
+    gapfree = lambda s: np.ascontiguousarray(s.reshape(s.shape[0], -1)[:, aw].T)  # noqa: E731
+    nsng = ref.norm(params, comp, hst['buckets'], span=1)
+    mus = geometry.convert2dev(scan['mu'][1] + scan['mu'][0], Cnt)
+    asng = ref.fprj(params, mus, span=1, att=1)[0]
+    rsn, _ = ref.randoms(params, hst['fansums'], span=1)
+    rsng = gapfree(rsn)
+    psng = gapfree(hst['psino'])
+    tab = mmrrec.subset_table(params)
+    an = asng * nsng
+    sens = np.stack([ref.bprj(params, an[tab[k, 1:]], tab[k, 1:], span=1)[0] for k in range(14)])
+    msk = geometry.get_cylinder(Cnt, rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
+    x = np.ones((320, 320, 127), np.float32)
+    ref.osem(params, x, msk, psng, rsng, np.zeros_like(rsng), nsng, asng, tab, sens, span=1)
+    d, q, ql = mmrrec.decay_quant_factors(hst, Cnt, comp)
+    want = geometry.convert2e7(x * np.float32(d * q * ql), Cnt)
+    rl2 = np.linalg.norm(out.im.astype(np.float64) - want) / np.linalg.norm(want)
+    assert rl2 <= 1e-4, f'span 1: relative L2 {rl2:.3e}'

@@ -70,8 +70,8 @@ def test_osemone_and_mmrchain_argument_checks(params):
         mmrrec.osemone({}, mu, hst, params, recmod=2)
     with pytest.raises(NotImplementedError, match='NIfTI'):
         mmrrec.osemone({}, mu, hst, params, recmod=1, store_img=True)
-    with pytest.raises(NotImplementedError, match='span-11'):
-        mmrrec.osemone({}, mu, hst, dict(params, Cnt=dict(params['Cnt'], SPN=1)), recmod=1)
+    with pytest.raises(ValueError, match='span'):
+        mmrrec.osemone({}, mu, hst, dict(params, Cnt=dict(params['Cnt'], SPN=3)), recmod=1)
     with pytest.raises(NotImplementedError, match='tAffine'):
         pipe.mmrchain({}, params, tAffine=[np.eye(4)])
     with pytest.raises(NotImplementedError, match='partial-volume'):
