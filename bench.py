@@ -3,7 +3,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload batch|osem|hist|diff|dynamic] [--replicates R]
 
-Workloads (seeded synthetic data; see DESIGN.md for the configuration they stand in for):
+Workloads (seeded synthetic data standing in for the phantom, list-mode and dynamic
+configurations, whose datasets are not available here):
   batch (default) batched bootstrap OSEM: R = 50 Poisson replicates of one synthetic scan
         (45 at 3e7 counts, 5 at 3e6), all reconstructed together per step: 14 sensitivity
         images + 4 iterations x 14 subsets, span-11 (837 x 252 x 344 sinograms),
