@@ -166,9 +166,12 @@ int nb_osem_subset_psf(nb_geom *g, float *img128, float *bimg128, const float *s
  *              chunk; 2 = 512 threads x 8 rays, 64/bs columns.  Results agree to rounding;
  *              batch.autotune picks (bs, tile) by timing them.
  * nb_to_batch / nb_from_batch convert nrep reference-layout images [nrep][320][320][127]
- * to and from that layout. */
+ * to and from that layout; nb_fill_batch sets every voxel of the nrep images in that layout
+ * to `value` (the OSEM start image) without a reference-layout source, zeroing the padding
+ * slot of each column and the images that pad the last group. */
 int nb_to_batch(float *dst, const float *src, int nrep, int bs, void *stream);
 int nb_from_batch(float *dst, const float *src, int nrep, int bs, void *stream);
+int nb_fill_batch(float *dst, float value, int nrep, int bs, void *stream);
 
 /* Forward and back projection of nrep images in the batched layout, one walk of the
  * geometry per bs images -- what gpu_fprj / gpu_bprj (prjf.cu:209-320, prjb.cu:190-308) do
@@ -256,8 +259,12 @@ int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag, cons
  * Limits: at most 4096 chunks in the plan (about 5e10 words); larger plans are rejected
  * with NB_ERR_ARG.  The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress, with the device current) and caches it, so make that first call
- * before any stream capture.  All calls on a device share the array and it keeps the last
- * call's tables; calls that overlap on the GPU race on it and must be serialised. */
+ * before any stream capture; the cached address belongs to that device's context, so it is
+ * stale after a cudaDeviceReset (do not call this after one).  The host arrays (LUTs and
+ * plan) are gathered into one host buffer and staged before the call returns, so the caller
+ * may reuse or free them at once, pinned or not.  All calls on a device share the array
+ * and it keeps the last call's tables; calls that overlap on the GPU race on it and must be
+ * serialised. */
 int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag,
                    const int *ele4chnk, const int *ele4thrd, int toff, int nitag, int tstart,
                    int tstop, int span, int btp, double btprt, uint64_t seed, int rep0, int nrep,

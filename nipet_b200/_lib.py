@@ -48,6 +48,7 @@ SIGNATURES = {
     'nb_putgaps': ([P, P, I, P, P], I),
     'nb_to_batch': ([P, P, I, I, P], I),
     'nb_from_batch': ([P, P, I, I, P], I),
+    'nb_fill_batch': ([P, C.c_float, I, I, P], I),
     'nb_osem_batch_subset': ([P, P, P, P, P, P, P, P, I, I, I, I, P, I, P], I),
     'nb_fprj_batch': ([P, P, P, I, I, I, P, I, P], I),
     'nb_bprj_batch': ([P, P, P, I, I, I, P, I, P], I),

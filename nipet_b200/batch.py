@@ -93,9 +93,9 @@ class BatchRecon:
             self.launches += 1
 
     def init_images(self, value: float = 1.0):
-        ones = torch.full((self.nrep, 320, 320, 127), value, device=self.device)
-        _lib.check(self.lib.nb_to_batch(dev_ptr(self.img), dev_ptr(ones), self.nrep, self.bs,
-                                        stream_ptr(self.device)))
+        """Every image set to `value` in place, in the batched layout (one fill kernel)."""
+        _lib.check(self.lib.nb_fill_batch(dev_ptr(self.img), float(value), self.nrep, self.bs,
+                                          stream_ptr(self.device)))
         self.launches += 1
 
     def subiteration(self, i: int, stream=None):

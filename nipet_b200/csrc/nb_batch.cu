@@ -14,6 +14,8 @@
 // backward-only mode is the batched projector pair (nb_fprj_batch / nb_bprj_batch).
 #include <math.h>
 
+#include <atomic>
+
 #include "nb_axial.cuh"
 #include "nb_internal.cuh"
 #include "nb_project.cuh"
@@ -553,6 +555,19 @@ __global__ void k_to_batch(float *__restrict__ dst, const float *__restrict__ sr
   }
 }
 
+// every voxel of the nrep images of the batched layout set to `value`; the padding slot of
+// each column (slot 127) and the images padding the last group set to zero
+__global__ void k_fill_batch(float *__restrict__ dst, float value, int nrep, int bs,
+                             size_t n) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % bs);
+    const int slot = (int)((t / bs) % NB_COLW);
+    const int g = (int)(t / ((size_t)bs * NB_COLW * NB_NCOL));
+    dst[t] = (g * bs + k < nrep && slot != NB_COLW - 1) ? value : 0.f;
+  }
+}
+
 __global__ void k_from_batch(float *__restrict__ dst, const float *__restrict__ src, int nrep,
                              int bs) {
   const size_t n = (size_t)nrep * NB_NCOL * NB_IMZ;
@@ -610,11 +625,13 @@ int launch_batch(nb_geom *g, const nbb::BatchArgs &a, cudaStream_t s) {
   static_assert(nbb::BSmem<BS, CH>::template misc_off<NOUT>() % 128 == 0, "misaligned barriers");
   static_assert(nbb::BSmem<BS, CH>::template total<NOUT>() <= 227 * 1024, "too much shared memory");
   const size_t smem = nbb::BSmem<BS, CH>::template total<NOUT>();
-  static bool set[64] = {false};
-  if (!set[g->device & 63]) {
+  // the shared-memory opt-in is set once per device and kernel shape; host threads may
+  // launch concurrently, so the flags are atomics (setting the attribute twice is harmless)
+  static std::atomic<bool> set[64];
+  if (!set[g->device & 63].load(std::memory_order_acquire)) {
     NB_CUDA(cudaFuncSetAttribute(nbb::k_osem_batch<BS, CH, NOUT, NT, RPT, MODE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    set[g->device & 63] = true;
+    set[g->device & 63].store(true, std::memory_order_release);
   }
   const long jobs = (long)a.nprj * a.ngroups;
   const int grid = jobs < g->nsm ? (int)jobs : g->nsm;
@@ -665,6 +682,14 @@ extern "C" int nb_to_batch(float *dst, const float *src, int nrep, int bs, void 
                           sizeof(float) * (size_t)((nrep + bs - 1) / bs) * bs * NB_NCOL * NB_COLW,
                           (cudaStream_t)stream));
   k_to_batch<<<4096, 256, 0, (cudaStream_t)stream>>>(dst, src, nrep, bs);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+extern "C" int nb_fill_batch(float *dst, float value, int nrep, int bs, void *stream) {
+  NB_REQUIRE(dst && nrep > 0 && (bs == 1 || bs == 2 || bs == 4), "nb_fill_batch: bad arguments");
+  const size_t n = (size_t)((nrep + bs - 1) / bs) * bs * NB_NCOL * NB_COLW;
+  k_fill_batch<<<4096, 256, 0, (cudaStream_t)stream>>>(dst, value, nrep, bs, n);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }
@@ -761,19 +786,16 @@ extern "C" int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128,
     if (st) return st;
   }
   NB_CUDA(cudaMemsetAsync(bimg128, 0, sizeof(float) * NB_IMG_COL128, s));
-  float *one = nullptr;  // the randoms factor of the single image
-  NB_CUDA(cudaMallocAsync((void **)&one, sizeof(float), s));
-  const float h_one = 1.f;  // a pageable-source async copy is staged before it returns
-  cudaError_t e = cudaMemcpyAsync(one, &h_one, sizeof(float), cudaMemcpyHostToDevice, s);
   int st = NB_OK;
-  if (e == cudaSuccess) {
+  cudaError_t e = cudaSuccess;
+  {
     nbb::BatchArgs a{};
     batch_geometry(g, a, 1, 1, 1, subs, nprj);
     a.img = krnl ? rm : img128;
     a.bimg = bimg128;
     a.psng = psng;
     a.rs = rs;
-    a.rscale = one;
+    a.rscale = g->d_one;  // the randoms factor of the single image
     st = launch_batch<1, 64, NB_NSN1, 1024, 4>(g, a, s);
     if (!st && krnl) st = nb_psf_col128(rm, bimg128, krnl, tmp, stream);
     if (!st) {
@@ -782,7 +804,6 @@ extern "C" int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128,
       e = cudaGetLastError();
     }
   }
-  cudaFreeAsync(one, s);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_osem_subset_span1", __FILE__, __LINE__);
   return st;
 }

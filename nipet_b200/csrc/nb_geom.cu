@@ -221,6 +221,7 @@ static void nb_geom_free(nb_geom *g) {
   cudaFree(g->d_bin1);
   cudaFree(g->d_scratch128);
   cudaFree(g->d_err);
+  cudaFree(g->d_one);
   free(g->h_s2c);
   free(g);
 }
@@ -399,8 +400,18 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
   ALLOC(g->d_bin1, sizeof(int16_t) * NB_NSN1);
   ALLOC(g->d_scratch128, sizeof(float) * NB_IMG_COL128);
   ALLOC(g->d_err, sizeof(int));
+  ALLOC(g->d_one, sizeof(float));
   ALLOC(d_tv, (size_t)naw * NB_N_TV);
 #undef ALLOC
+  {
+    const float one = 1.f;
+    if (cudaMemcpy(g->d_one, &one, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      nb_set_error_msg("nb_geom_create: upload of a constant failed");
+      st = NB_ERR_CUDA;
+      goto fail;
+    }
+  }
   if (cudaMemset(g->d_err, 0, sizeof(int)) != cudaSuccess ||
       cudaMemset(g->d_scol, 0, sizeof(int32_t) * (size_t)naw * NB_STEP_STRIDE) != cudaSuccess ||
       cudaMemset(g->d_st, 0, sizeof(float) * (size_t)naw * NB_STEP_STRIDE) != cudaSuccess ||

@@ -966,25 +966,23 @@ extern "C" int nb_hist_static(const int32_t *lm, int64_t ele, int nchnk, const i
   a.atag = reinterpret_cast<const int64_t *>(base + kAtagOff);
   a.e4c = reinterpret_cast<const int *>(base + kE4cOff);
   a.e4t = reinterpret_cast<const int *>(base + kE4tOff);
-  const size_t nsn = (size_t)NB_NSN1 * sizeof(int16_t);
-  cudaError_t e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_sn11), sn1_sn11, nsn,
-                                  cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_ssrb), sn1_ssrb, nsn,
-                        cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kLutOff + offsetof(HistLUT, sn1_rno), sn1_rno, 2 * nsn,
-                        cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kS2cOff, s2cF, (size_t)NB_NSBINANG * sizeof(short2),
-                        cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kAtagOff, atag, sizeof(int64_t) * nchnk, cudaMemcpyHostToDevice,
-                        s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kE4cOff, ele4chnk, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kE4tOff, ele4thrd, sizeof(int) * nchnk, cudaMemcpyHostToDevice, s);
+  // The caller's host arrays are first gathered into one pageable host buffer, laid out as
+  // the static array, and moved with one copy: a cudaMemcpyAsync from pageable memory has
+  // staged its source before it returns, so the caller may reuse or free its arrays (pinned
+  // ones included) as soon as this call returns, as with nb_hist.  Only host memory is
+  // allocated here.
+  const size_t used = kE4tOff + sizeof(int) * (size_t)nchnk;
+  std::vector<unsigned char> h(used, 0);
+  HistLUT hl;
+  memcpy(hl.sn1_sn11, sn1_sn11, sizeof(hl.sn1_sn11));
+  memcpy(hl.sn1_ssrb, sn1_ssrb, sizeof(hl.sn1_ssrb));
+  memcpy(hl.sn1_rno, sn1_rno, sizeof(hl.sn1_rno));
+  memcpy(&h[kLutOff], &hl, sizeof(HistLUT));
+  memcpy(&h[kS2cOff], s2cF, (size_t)NB_NSBINANG * sizeof(short2));
+  memcpy(&h[kAtagOff], atag, sizeof(int64_t) * nchnk);
+  memcpy(&h[kE4cOff], ele4chnk, sizeof(int) * nchnk);
+  memcpy(&h[kE4tOff], ele4thrd, sizeof(int) * nchnk);
+  cudaError_t e = cudaMemcpyAsync(base, h.data(), used, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = launch_hist(a, reinterpret_cast<unsigned *>(base + kCtrOff), s);
   if (e != cudaSuccess) return nb_cuda_fail(e, "nb_hist_static", __FILE__, __LINE__);
   return NB_OK;

@@ -37,6 +37,7 @@ struct nb_geom {
   float maxseg;          // longest walk segment of the geometry (cm)
   int fxbits;            // fixed-point headroom of the backward accumulators
   int *d_err;            // device error flag
+  float *d_one;          // the constant 1.0f (randoms factor of a single-image batch)
   // host copies of the LUTs (for nb_geom_tables)
   float h_crs[504 * 4];
   int16_t *h_s2c;

@@ -2,6 +2,8 @@
 // the sinogram gap kernels.  The projector kernel itself is in nb_project.cuh.
 #include <math.h>
 
+#include <atomic>
+
 #include "nb_axial.cuh"
 #include "nb_internal.cuh"
 #include "nb_project.cuh"
@@ -98,11 +100,12 @@ __global__ void k_count_reads(const float4 *__restrict__ hdr, const float *__res
 template <int MODE, int CH>
 int launch_project(nb_geom *g, const PrjArgs &a, cudaStream_t stream) {
   const size_t smem = Smem<MODE, CH>::total;
-  static bool attr_set[64] = {false};
-  if (!attr_set[g->device & 63]) {
+  // set once per device and kernel shape; atomics, since host threads may launch at once
+  static std::atomic<bool> attr_set[64];
+  if (!attr_set[g->device & 63].load(std::memory_order_acquire)) {
     NB_CUDA(cudaFuncSetAttribute(k_project<MODE, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-    attr_set[g->device & 63] = true;
+    attr_set[g->device & 63].store(true, std::memory_order_release);
   }
   if (a.nprj <= 0) return NB_OK;
   const int grid = a.nprj < g->nsm ? a.nprj : g->nsm;

@@ -170,6 +170,12 @@ class Recon:
             raise ValueError(f'unrecognised span {span}')
         self.span = int(span)
         self.nsn = 837 if self.span == 11 else 4084
+        # every sinogram is read over NAW x nsn elements on the device: check the shapes
+        # before anything is copied or launched
+        for a, nm in ((psng, 'psng'), (rsng, 'rsng'), (nsng, 'nsng'), (asng, 'asng'),
+                      (ssng, 'ssng')):
+            if a is not None and tuple(np.shape(a)) != (NAW, self.nsn):
+                raise ValueError(f'{nm} must have shape {(NAW, self.nsn)} at span {self.span}')
         self.device = torch.device(device or 'cuda')
         self.params = params
         self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
@@ -186,10 +192,6 @@ class Recon:
         self.subs = [torch.from_numpy(tab[i, 1:]).to(dev) for i in range(self.nsub)]
         self.msk128 = geometry.cylinder_mask128(params['Cnt'], mask_radius, dev)
         st = stream_ptr(dev)
-        for a, nm in ((self.psng, 'psng'), (self.rsng, 'rsng'), (self.nsng, 'nsng'),
-                      (self.asng, 'asng')):
-            if tuple(a.shape) != (NAW, self.nsn):
-                raise ValueError(f'{nm} must have shape {(NAW, self.nsn)} at span {self.span}')
         self.rs = torch.empty((NAW, self.nsn), device=dev)
         _lib.check(self.lib.nb_osem_rs(dev_ptr(self.rs), dev_ptr(self.rsng),
                                        dev_ptr(self.ssng) if self.ssng is not None else None,

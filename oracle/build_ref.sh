@@ -2,12 +2,20 @@
 # Compile the reference's own CUDA projectors, OSEM, list-mode histogrammer and randoms, normalisation (sources read in place from the
 # reference tree, nothing copied) with the test-only harness oracle/ref_harness.cu into
 # oracle/_ref/libnipet_ref.so.  Flags follow the reference's Release build (-O3, no fast
-# math), for sm_100a.  Usage: oracle/build_ref.sh [reference root]
+# math), for sm_100a.
+# Usage: oracle/build_ref.sh [reference root]
+# The reference root is the argument, else $NIPET_REFERENCE, else the checkout location of
+# the build container (/root/reference).  Without a reference tree there nothing is built
+# and the script exits 0 (a machine without the checkout uses a prebuilt oracle/_ref).
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-/root/reference}/niftypet/nipet
+ROOT=${1:-${NIPET_REFERENCE:-/root/reference}}
+REF=$ROOT/niftypet/nipet
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
-[ -d "$REF/prj/src" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
+if [ ! -d "$REF/prj/src" ]; then
+  echo "build_ref.sh: no reference sources under $ROOT; oracle/_ref not rebuilt" >&2
+  exit 0
+fi
 mkdir -p "$HERE/_ref"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++14 -Xcompiler -fPIC -shared \
   -DNIPET_CU_THREADS=1024 -I"$REF/include" -I"$REF/prj/src" -I"$REF/lm/src" -I"$REF/src" \

@@ -1,9 +1,9 @@
-"""Small, self-contained GPU cases for profiling the hot kernels with Nsight Compute.
+"""Benchmark infrastructure beside bench.py: small, self-contained GPU cases for profiling the hot kernels with Nsight Compute.
 
-    python -m nipet_b200.profile_cases projectors   # k_project: back, forward, fused OSEM
-    python -m nipet_b200.profile_cases hist         # k_hist on a 20M-word stream
-    python -m nipet_b200.profile_cases hist200      # k_hist on the 2e8-word, 600 s stream
-    python -m nipet_b200.profile_cases hist200boot  # the same with 4 Poisson replicates
+    python profile_cases.py projectors   # k_project: back, forward, fused OSEM
+    python profile_cases.py hist         # k_hist on a 20M-word stream
+    python profile_cases.py hist200      # k_hist on the 2e8-word, 600 s stream
+    python profile_cases.py hist200boot  # the same with 4 Poisson replicates
 
 `projectors` builds the geometry, a phantom image (col128 layout), subset 3 of 14 and random
 prompt / (r+s)/(an) / a*n sinograms (~0.8 GB on the device), then launches the back projection
@@ -11,7 +11,7 @@ prompt / (r+s)/(an) / a*n sinograms (~0.8 GB on the device), then launches the b
 launches 15, 16, 17 are one warm launch of each mode:
 
     ncu --set full --clock-control none -k regex:k_project -s 15 -c 3 -o prof \\
-        python -m nipet_b200.profile_cases projectors
+        python profile_cases.py projectors
 
 `hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2);
 `hist200` does the same on the full-size 2e8-word stream over 600 s (1.2 GB on the device);
@@ -24,14 +24,19 @@ launches 0, 1 are width 4, 2, 3 width 2 -- use -s 1 -c 1 and -s 3 -c 1).
 """
 from __future__ import annotations
 
+import os
 import sys
 
 import torch
 
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
 
 def projectors(device='cuda:0'):
-    from . import _lib, geometry, petprj, phantoms
-    from .device import dev_ptr, get_geometry, stream_ptr
+    from nipet_b200 import _lib, geometry, petprj, phantoms
+    from nipet_b200.device import dev_ptr, get_geometry, stream_ptr
     dev = torch.device(device)
     p = geometry.get_mmrparams()
     g = get_geometry(p['txLUT'], p['axLUT'], dev)
@@ -63,7 +68,7 @@ def projectors(device='cuda:0'):
 
 
 def hist(device='cuda:0', nwords=20_000_000, duration=60, nrep=1):
-    from . import geometry, mmr_lmproc, phantoms
+    from nipet_b200 import geometry, mmr_lmproc, phantoms
     dev = torch.device(device)
     p = geometry.get_mmrparams()
     lm = phantoms.lm_stream_fast(nwords, duration, params=p, seed=0, device=dev)
@@ -78,8 +83,8 @@ def hist(device='cuda:0', nwords=20_000_000, duration=60, nrep=1):
 
 
 def batch(device='cuda:0'):
-    from . import batch as B
-    from . import geometry
+    from nipet_b200 import batch as B
+    from nipet_b200 import geometry
     dev = torch.device(device)
     p = geometry.get_mmrparams()
     gen = torch.Generator(device=dev).manual_seed(0)

@@ -9,8 +9,9 @@ extracts `axial_lut`, `transaxial_lut` (`niftypet/nipet/mmraux.py`) and
 The scanner constants (`Cnt`) come from the un-vendored `ninst` package in the
 reference; the values used here are `nipet_b200.geometry.get_mmr_constants()`.
 
-Run from the repository root, in a container that has the reference checkout:
-    python tests/golden/make_lut_golden.py /root/reference
+Run from the repository root, in a container that has the reference checkout, giving
+its root as the argument or in NIPET_REFERENCE:
+    python tests/golden/make_lut_golden.py <reference root>
 """
 import ast
 import logging
@@ -59,4 +60,7 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('NIPET_REFERENCE')
+    if not root:
+        sys.exit('usage: make_lut_golden.py <reference root> (or set NIPET_REFERENCE)')
+    main(root)

@@ -109,3 +109,20 @@ def test_layout_conversions_on_tensors_match_numpy(params):
     back = geometry.convert2e7(dev, params['Cnt'])
     back_t = geometry.convert2e7(torch.from_numpy(dev), params['Cnt'])
     assert np.array_equal(back, back_t.numpy())
+
+
+@pytest.mark.parametrize('span,bad', [(1, 'ssng'), (1, 'rsng'), (11, 'ssng')])
+def test_recon_rejects_mismatched_sinograms(params, span, bad):
+    """Every sinogram a Recon reads on the device must be [68516, nsinos] of its span; a
+    span-11 scatter sinogram given to a span-1 reconstruction is refused before any copy
+    or launch (the kernels would read past its end)."""
+    nsn = 837 if span == 11 else 4084
+    other = 4084 if span == 11 else 837
+    shp = {k: (68516, nsn) for k in ('psng', 'rsng', 'nsng', 'asng', 'ssng')}
+    shp[bad] = (68516, other)
+    # shape-only stand-ins: the check must fire before any element is read
+    arr = {k: np.lib.stride_tricks.as_strided(np.zeros(1, np.float32), v, (0, 0))
+           for k, v in shp.items()}
+    with pytest.raises(ValueError, match=bad):
+        mmrrec.Recon(params, arr['psng'], arr['rsng'], arr['nsng'], arr['asng'],
+                     ssng=arr['ssng'], device='cpu', span=span)
