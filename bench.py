@@ -400,26 +400,52 @@ def run_batch(args, ws, rank, dev):
     launches_per_step = br.launches // args.steps
     t_step = _max_over_ranks(float(np.mean(times)), ws, dev)
     value = ws * nrep / t_step
-    # roofline: one graph replay = 14 k_osem_batch launches + 14 image updates (the update
-    # kernels are ~1% of the replay); achieved = algorithmic bytes of the 14 launches / time
+    # roofline of the dominant kernel, k_osem_batch (one graph replay = 14 of its launches +
+    # 14 image updates, ~1% of the replay).  Its binding resource is the shared-memory
+    # pipe: every Siddon voxel read/update is served from image columns staged in shared
+    # memory, each staged column serving ~35 rays.  achieved = shared-memory wavefronts of
+    # one launch (ncu count of the 8-image capture of this kernel shape -- 2 groups of 4 --
+    # scaled by the number of 4-image groups, since every group walks every LOR) over the
+    # launch's live CUDA-event time; peak = one wavefront per cycle per SM at the sampled
+    # clock.  Beside it: real DRAM traffic (ncu dram bytes, scaled the same way) against the
+    # measured HBM bandwidth, and the algorithmic bytes (4 B per voxel read/update as if
+    # from HBM) against the same peak.
     t_it = float(np.mean(it_ms)) / 1e3
-    achieved = bytes_iter / t_it / 1e9
+    t_launch = t_it / len(br.subs)
+    achieved_alg = bytes_iter / t_it / 1e9
     peak, peak_kind = _peaks()
+    gscale = ngroups / 2.0 if br.bs == 4 else None
     tr8 = _traffic('osem_batch_8img')
-    traffic = None if tr8 is None else tr8 * nrep / 8.0
-    # the on-chip bound: shared-memory wavefronts of one launch (ncu count of the 8-image
-    # capture, scaled by images) over the live launch time, against one wavefront per
-    # cycle per SM at the sampled clock
     wf8 = _traffic('osem_batch_8img_smem_wavefronts')
-    onchip = None
-    if wf8:
-        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
-        mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
-        ach = wf8 * nrep / 8.0 / (t_it / len(br.subs))
-        onchip = {'bound': 'shared-memory pipe', 'unit': 'wavefronts/s', 'achieved': ach,
-                  'peak': nsm * mhz * 1e6, 'frac': ach / (nsm * mhz * 1e6),
-                  'wavefronts_per_launch': wf8 * nrep / 8.0,
-                  'peak_basis': f'1 wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz'}
+    traffic = None if (tr8 is None or gscale is None) else tr8 * gscale
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+    smem_peak = nsm * mhz * 1e6
+    kernel = (f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk, tile {br.tile}, '
+              f'{ngroups} image groups per launch)')
+    if wf8 and gscale is not None:
+        wf = wf8 * gscale
+        roof = {'bound': 'smem', 'achieved': wf / t_launch, 'peak': smem_peak,
+                'unit': 'wavefronts/s', 'frac': wf / t_launch / smem_peak,
+                'peak_kind': f'1 shared-memory wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} '
+                             'MHz (median sampled clock)',
+                'traffic': traffic, 'kernel': kernel, 'wavefronts_per_launch': wf,
+                'launch_ms_avg': t_launch * 1e3}
+    else:  # no capture of this shape: the algorithmic HBM figure is all there is
+        roof = {'bound': 'hbm', 'achieved': achieved_alg, 'peak': peak, 'unit': 'GB/s',
+                'frac': achieved_alg / peak, 'peak_kind': peak_kind, 'traffic': traffic,
+                'kernel': kernel, 'launch_ms_avg': t_launch * 1e3}
+    roof['hbm'] = {'unit': 'GB/s', 'peak': peak, 'peak_kind': peak_kind,
+                   'achieved': None if traffic is None else traffic / t_launch / 1e9,
+                   'frac': None if traffic is None else traffic / t_launch / 1e9 / peak,
+                   'source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum per launch '
+                             '(8-image capture x groups / 2) over the live launch time'}
+    roof['algorithmic'] = {'unit': 'GB/s', 'bytes_per_launch': bytes_iter / len(br.subs),
+                           'achieved': achieved_alg, 'frac_of_hbm_peak': achieved_alg / peak,
+                           'note': '4 B per Siddon voxel read and per back-projection '
+                                   'update, per image, as if every one came from HBM, + '
+                                   'sinogram rows; above 1 because staged columns are '
+                                   'reused from shared memory'}
 
     # e2e through the public batch API: pinned host prompts -> device, reconstruction,
     # voxel-wise mean/std images back to the host
@@ -465,17 +491,7 @@ def run_batch(args, ws, rank, dev):
 
     res = {
         'ms_per_step': t_step * 1e3, 'value': value, 'e2e': e2e, 'clocks': clocks,
-        'gpu_launches': launches_per_step, 'plain_dropin': plain,
-        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                     'frac': achieved / peak, 'traffic': traffic,
-                     'kernel': f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk, '
-                               f'tile {br.tile})',
-                     'peak_kind': peak_kind, 'bytes_per_launch_avg': bytes_iter / len(br.subs),
-                     'launch_ms_avg': t_it * 1e3 / len(br.subs),
-                     'note': 'achieved counts 4 B per Siddon voxel read/update as if from HBM; '
-                             'the kernel stages image columns in shared memory and reuses each '
-                             'about 35 times, so its bound is on-chip (see onchip)',
-                     'onchip': onchip},
+        'gpu_launches': launches_per_step, 'plain_dropin': plain, 'roofline': roof,
         'config': {'workload': f'batched bootstrap OSEM, {nrep} replicates '
                                f'({nrep - nlow} at 3e7, {nlow} at 3e6 counts), span-11 '
                                f'837x252x344, 320x320x127 f32, 4 it x 14 subsets + '
@@ -830,10 +846,10 @@ def _norm_components(seed=12):
             'dtp': u(-3e-6, -1e-6, 64), 'dtnp': u(1e-7, 4e-7, 64)}
 
 
-def _chain_inputs(args, params, dev, seed):
+def _chain_inputs(args, params, dev, seed, project=None):
     from nipet_b200 import geometry, phantoms
     lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=seed,
-                                 device=dev)
+                                 device=dev, project=project)
     muo = geometry.convert2e7(phantoms.water_mumap(), params['Cnt'])
     return lm, [np.zeros_like(muo), muo], _norm_components()
 
@@ -931,6 +947,19 @@ def run_chain(args, ws, rank, dev):
 # reference arm: NIPET has no CPU path; its algorithm restated as the FP64 oracle on the
 # host cores (bounded samples of the same workload)
 # ---------------------------------------------------------------------------------------
+def _ref_projector(params, dev):
+    """`project(img, span, att)` for the synthetic-data builders made from the reference's
+    own gpu_fprj (oracle/_ref), so that the reference arm's inputs come from the reference
+    build and torch alone, without this package's library."""
+    import torch
+    from oracle import ref
+
+    def project(img, span, att):
+        x = img.detach().cpu().numpy() if isinstance(img, torch.Tensor) else img
+        return torch.from_numpy(ref.fprj(params, x, None, span=span, att=att)[0]).to(dev)
+    return project
+
+
 def _reference_cuda_recon(params, scan_host, tab, msk):
     """One replicate through the reference's own CUDA build (oracle/_ref): 14 gpu_bprj
     sensitivity images and 4 osem() iterations with host arrays, as mmrrec.osemone drives
@@ -946,6 +975,55 @@ def _reference_cuda_recon(params, scan_host, tab, msk):
         ref.osem(params, img, msk, h['psng'], h['rsng'], h['ssng'], h['nsng'], h['asng'], tab,
                  sens)
     return time.perf_counter() - t
+
+
+def _reference_hist(args, params, steps, warmup):
+    """The reference's lmproc (oracle/_ref) on the synthetic list-mode stream written to a
+    file (its input): span 11, span 1 and 10 Poisson bootstrap calls per step."""
+    import torch
+    from nipet_b200 import phantoms
+    from oracle import ref
+    dev = torch.device('cuda', 0)
+    unit = METRIC['hist'][1]
+    lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=0,
+                                 device=dev, project=_ref_projector(params, dev)
+                                 ).cpu().numpy()
+    torch.cuda.empty_cache()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, 'lm.bf')
+        lm.astype('<i4').tofile(path)
+        ts = []
+        for _ in range(warmup + steps):
+            t = time.perf_counter()
+            ref.hist(params, path, span=11)
+            ref.hist(params, path, span=1)
+            for _ in range(10):  # the reference draws one bootstrap replicate per call
+                ref.hist(params, path, span=11, btp=2, btprt=1.0)
+            ts.append(time.perf_counter() - t)
+    v = lm.size / float(np.mean(ts[warmup:]))
+    sample = (f'{lm.size} words over {args.duration} s per step through the reference CUDA '
+              'build (lmproc: file read, chunking, gpu_hst): span 11, span 1 and 10 '
+              'Poisson bootstrap replicates (span 11), on this GPU')
+    return {'value': v, 'n_gpus': 1, 'ms_per_step': lm.size / v * 1e3, 'dtype': 'u32',
+            'steps': steps, 'warmup': warmup,
+            'config': {'workload': 'hist', 'implementation':
+                       'reference CUDA (oracle/_ref), compiled for sm_100a'},
+            'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1, 'kind': 'reference',
+                             'sample': sample}}
+
+
+def _native_libraries():
+    """Shared libraries of this repository mapped into the process (from /proc/self/maps)."""
+    libs = set()
+    try:
+        with open('/proc/self/maps') as f:
+            for ln in f:
+                path = ln.split()[-1] if ln.strip() else ''
+                if path.endswith('.so') and path.startswith(ROOT):
+                    libs.add(os.path.relpath(path, ROOT))
+    except OSError:
+        return None
+    return sorted(libs)
 
 
 def run_reference(args):
@@ -972,40 +1050,15 @@ def run_reference(args):
     except Exception:
         use_cuda = False
     if use_cuda and args.workload == 'hist':
-        import torch
-        from nipet_b200 import phantoms
-        from oracle import ref
-        dev = torch.device('cuda', 0)
-        lm = phantoms.lm_stream_fast(args.events, args.duration, params=params, seed=0,
-                                     device=dev).cpu().numpy()
-        with tempfile.TemporaryDirectory() as td:
-            path = os.path.join(td, 'lm.bf')
-            lm.astype('<i4').tofile(path)
-            ts = []
-            for _ in range(args.warmup + args.steps):
-                t = time.perf_counter()
-                ref.hist(params, path, span=11)
-                ref.hist(params, path, span=1)
-                for _ in range(10):  # the reference draws one bootstrap replicate per call
-                    ref.hist(params, path, span=11, btp=2, btprt=1.0)
-                ts.append(time.perf_counter() - t)
-        v = lm.size / float(np.mean(ts[args.warmup:]))
-        sample = (f'{lm.size} words over {args.duration} s per step through the reference CUDA '
-                  'build (lmproc: file read, chunking, gpu_hst): span 11, span 1 and 10 '
-                  'Poisson bootstrap replicates (span 11), on this GPU')
-        line.update({'value': v, 'n_gpus': 1, 'ms_per_step': lm.size / v * 1e3,
-                     'dtype': 'u32',
-                     'config': {'workload': 'hist', 'implementation':
-                                'reference CUDA (oracle/_ref), compiled for sm_100a'},
-                     'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
-                                      'kind': 'reference', 'sample': sample}})
+        line.update(_reference_hist(args, params, args.steps, args.warmup))
     elif use_cuda and args.workload == 'chain':
         import torch
         from nipet_b200 import geometry as G
         from nipet_b200 import mmrhist, mmrrec
         from oracle import ref
         dev = torch.device('cuda', 0)
-        lm_d, mu, comp = _chain_inputs(args, params, dev, 0)
+        lm_d, mu, comp = _chain_inputs(args, params, dev, 0,
+                                       project=_ref_projector(params, dev))
         lm = lm_d.cpu().numpy()
         del lm_d
         Cnt = params['Cnt']
@@ -1086,7 +1139,8 @@ def run_reference(args):
         from nipet_b200 import dynamic, mmrrec
         from oracle import ref
         dev = torch.device('cuda', 0)
-        sc = dynamic.dynamic_scan(params, dev, [3e6], seed=0)
+        sc = dynamic.dynamic_scan(params, dev, [3e6], seed=0,
+                                  project=_ref_projector(params, dev))
         an, nsng = sc['an'].cpu().numpy(), sc['nsng'].cpu().numpy()
         psng = sc['psng'][0].cpu().numpy()
         asng = np.where(np.abs(nsng) > 0, an / np.where(nsng == 0, 1, nsng), 0).astype(np.float32)
@@ -1126,7 +1180,7 @@ def run_reference(args):
         import torch
         from nipet_b200 import mmrrec
         dev = torch.device('cuda', 0)
-        scan = mmrrec.synthetic_scan(params, dev, seed=0)
+        scan = mmrrec.synthetic_scan(params, dev, seed=0, project=_ref_projector(params, dev))
         host = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
         del scan
         torch.cuda.empty_cache()
@@ -1145,6 +1199,12 @@ def run_reference(args):
                                 'reference CUDA (oracle/_ref), compiled for sm_100a'},
                      'cpu_baseline': {'value': v, 'unit': unit, 'cores': 1,
                                       'kind': 'reference', 'sample': sample}})
+        if args.workload == 'batch' and args.hist_steps > 0:
+            h = _reference_hist(args, params, 1, 1)
+            h['metric'], h['unit'] = METRIC['hist']
+            h['e2e'] = {'value': h['value'], 'unit': h['unit'], 'h2d_bytes_per_step': 0,
+                        'd2h_bytes_per_step': 0}
+            line['hist'] = h
     else:
         vals = []
         if args.workload in ('osem', 'batch', 'diff', 'dynamic'):
@@ -1178,6 +1238,7 @@ def run_reference(args):
                      'cpu_baseline': cb})
     line['e2e'] = {'value': line['value'], 'unit': unit, 'h2d_bytes_per_step': 0,
                    'd2h_bytes_per_step': 0}
+    line['native_libraries'] = _native_libraries()
     return line
 
 
@@ -1197,6 +1258,9 @@ def main():
     ap.add_argument('--events', type=int, default=200_000_000)
     ap.add_argument('--duration', type=int, default=600)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--hist-steps', type=int, default=10,
+                    help='timed steps of the list-mode histogram measured after the batch '
+                         'workload (its `hist` sub-object; 0 = skip)')
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if (args.workload == 'hist' and args.impl == 'ours') else 3
@@ -1214,6 +1278,19 @@ def main():
     run = {'batch': run_batch, 'osem': run_osem, 'hist': run_hist, 'diff': run_diff,
            'dynamic': run_dynamic, 'chain': run_chain}[args.workload]
     res = run(args, ws, rank, dev)
+    hist = None
+    if args.workload == 'batch' and args.hist_steps > 0:
+        # the list-mode hot path, measured in the same process after the batch workload
+        import copy
+        torch.cuda.empty_cache()
+        ha = copy.copy(args)
+        ha.steps, ha.warmup, ha.e2e_steps = args.hist_steps, max(3, min(args.warmup, 5)), 1
+        h = run_hist(ha, ws, rank, dev)
+        hist = {'metric': METRIC['hist'][0], 'value': h['value'], 'unit': METRIC['hist'][1],
+                'steps': ha.steps, 'warmup': ha.warmup, 'ms_per_step': h['ms_per_step'],
+                'dtype': 'u32', 'config': h['config'], 'roofline': h['roofline'],
+                'cpu_baseline': h.get('cpu_baseline'), 'e2e': h['e2e'],
+                'gpu_launches': h['gpu_launches'], 'clocks': h['clocks']}
     metric, unit = METRIC[args.workload]
     if rank == 0:
         line = {'metric': metric, 'value': res['value'], 'unit': unit, 'n_gpus': ws,
@@ -1225,6 +1302,8 @@ def main():
                 'gpu_launches': res['gpu_launches'], 'clocks': res['clocks']}
         if res.get('plain_dropin') is not None:
             line['plain_dropin'] = res['plain_dropin']
+        if hist is not None:
+            line['hist'] = hist
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

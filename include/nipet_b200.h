@@ -286,6 +286,16 @@ int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t 
  * memory of calls still in flight on a stream stays until they finish. */
 int nb_hist_trim(void);
 
+/* ---- host -> device transfer ----------------------------------------------------------
+ * nb_copy_h2d replaces the per-call pageable cudaMemcpy of the host arrays petprj.osem,
+ * fprj and bprj receive (prj/src/prj_module.cu:613-839 -> recon.cu:334-419, and the
+ * sinogram/image uploads of prj_module.cu:232-608): `bytes` from pageable host memory `src`
+ * to device memory `dst`, through a ring of pinned staging buffers (allocated on the first
+ * call on a device, kept until exit) filled by several host threads while the DMA of the
+ * previous chunk runs.  Returns once `src` has been read entirely (the caller may reuse it);
+ * the copies are ordered on `stream`.  Calls on one device are serialised. */
+int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,7 @@ SIGNATURES = {
     'nb_hist_unpack':([P, C.c_size_t, P, P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                         P], I),
     'nb_hist_trim': ([], I),
+    'nb_copy_h2d': ([P, P, C.c_size_t, P], I),
     'nb_osem_subset_span1': ([P, P, P, P, P, P, P, P, I, P, P, P], I),
 }
 

@@ -1,0 +1,102 @@
+// nb_stage.cu -- host -> device copies of large pageable host arrays through pinned staging
+// buffers, the host CPU copy split over several threads.
+//
+// The drop-in operators take host (numpy) arrays like the reference's petprj, whose
+// osem_rec copies ~1.8 GB of sinograms and sensitivity images from pageable memory on
+// every call (prj/src/prj_module.cu:613-839, recon.cu:334-419).  A pageable cudaMemcpy goes
+// through one driver-side bounce buffer filled by one CPU thread.  Here each chunk of the
+// source is copied into one of a ring of pinned buffers by several host threads at once
+// while the DMA engine moves the previous chunk, so the copy runs at the speed of a
+// multi-threaded memcpy instead of a single-threaded one.
+//
+// The staging ring (NB_STAGE_SLOTS pinned buffers of NB_STAGE_CHUNK bytes) is allocated on
+// the first call on a device and kept until the process exits.  Calls on one device are
+// serialised by a mutex.  Like a pageable-source cudaMemcpyAsync, a call returns once the
+// whole source has been read into staging memory (the caller may reuse it at once); the
+// DMAs themselves are ordered on the caller's stream.
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "nb_internal.cuh"
+
+#define NB_STAGE_SLOTS 4
+#define NB_STAGE_CHUNK ((size_t)32 << 20)
+
+namespace {
+
+struct Stage {
+  unsigned char *buf[NB_STAGE_SLOTS] = {};
+  cudaEvent_t done[NB_STAGE_SLOTS] = {};
+  bool ready = false;
+  std::mutex mu;
+};
+
+Stage g_stage[64];
+std::mutex g_init_mu;
+
+int stage_init(Stage &s) {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (s.ready) return NB_OK;
+  for (int k = 0; k < NB_STAGE_SLOTS; k++) {
+    NB_CUDA(cudaHostAlloc((void **)&s.buf[k], NB_STAGE_CHUNK, cudaHostAllocPortable));
+    NB_CUDA(cudaEventCreateWithFlags(&s.done[k], cudaEventDisableTiming));
+  }
+  s.ready = true;
+  return NB_OK;
+}
+
+// memcpy of n bytes split over nthr threads (the calling thread takes the last part)
+void par_copy(unsigned char *dst, const unsigned char *src, size_t n, int nthr) {
+  if (nthr <= 1 || n < ((size_t)1 << 20)) {
+    memcpy(dst, src, n);
+    return;
+  }
+  const size_t part = ((n / nthr) + 4095) & ~(size_t)4095;
+  std::vector<std::thread> th;
+  size_t off = 0;
+  for (int t = 0; t < nthr - 1 && off < n; t++) {
+    const size_t len = off + part < n ? part : n - off;
+    th.emplace_back([=] { memcpy(dst + off, src + off, len); });
+    off += len;
+  }
+  if (off < n) memcpy(dst + off, src + off, n - off);
+  for (auto &x : th) x.join();
+}
+
+int copy_threads() {
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int n = hc == 0 ? 4 : (int)hc;
+  return n > 8 ? 8 : n;
+}
+
+}  // namespace
+
+extern "C" int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *stream) {
+  NB_REQUIRE(bytes == 0 || (dst && src), "nb_copy_h2d: NULL pointer");
+  if (bytes == 0) return NB_OK;
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_REQUIRE(dev >= 0 && dev < 64, "nb_copy_h2d: device index above 63");
+  Stage &s = g_stage[dev];
+  int st = stage_init(s);
+  if (st) return st;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const int nthr = copy_threads();
+  std::lock_guard<std::mutex> lk(s.mu);
+  unsigned char *d = static_cast<unsigned char *>(dst);
+  const unsigned char *h = static_cast<const unsigned char *>(src);
+  int slot = 0;
+  for (size_t off = 0; off < bytes; off += NB_STAGE_CHUNK) {
+    const size_t n = bytes - off < NB_STAGE_CHUNK ? bytes - off : NB_STAGE_CHUNK;
+    // the slot's previous DMA (this call's or an earlier one's) must have left the buffer
+    NB_CUDA(cudaEventSynchronize(s.done[slot]));
+    par_copy(s.buf[slot], h + off, n, nthr);
+    NB_CUDA(cudaMemcpyAsync(d + off, s.buf[slot], n, cudaMemcpyHostToDevice, cs));
+    NB_CUDA(cudaEventRecord(s.done[slot], cs));
+    slot = (slot + 1) % NB_STAGE_SLOTS;
+  }
+  return NB_OK;
+}

@@ -12,7 +12,8 @@ import torch
 
 from . import _lib
 
-__all__ = ['Geometry', 'get_geometry', 'to_device', 'dev_ptr', 'stream_ptr', 'device_of']
+__all__ = ['Geometry', 'get_geometry', 'to_device', 'dev_ptr', 'stream_ptr', 'device_of',
+           'projector']
 
 
 def device_of(Cnt: dict | None = None, device=None) -> torch.device:
@@ -37,10 +38,23 @@ _NP2TORCH = {np.dtype('float32'): torch.float32, np.dtype('float64'): torch.floa
              np.dtype('uint32'): torch.uint32, np.dtype('int8'): torch.int8}
 
 
+# host arrays at least this large go through nb_copy_h2d (multi-threaded pinned staging)
+STAGED_COPY_BYTES = 8 << 20
+
+
 def to_device(x, dtype, device: torch.device, copy: bool = False) -> torch.Tensor:
     """Contiguous device tensor view (or copy) of a numpy array, torch tensor, or any
-    object exposing `__cuda_array_interface__` / DLPack."""
+    object exposing `__cuda_array_interface__` / DLPack.  Large host arrays already in
+    `dtype` are copied by `nb_copy_h2d`."""
     tdt = _NP2TORCH[np.dtype(dtype)]
+    dev = torch.device(device)
+    if (isinstance(x, np.ndarray) and x.dtype == np.dtype(dtype) and x.flags.c_contiguous
+            and x.nbytes >= STAGED_COPY_BYTES and dev.type == 'cuda'):
+        t = torch.empty(x.shape, dtype=tdt, device=dev)
+        with torch.cuda.device(dev):
+            _lib.check(_lib.load().nb_copy_h2d(dev_ptr(t), x.ctypes.data_as(C.c_void_p),
+                                               x.nbytes, stream_ptr(dev)))
+        return t
     if isinstance(x, torch.Tensor):
         t = x
     elif isinstance(x, np.ndarray):
@@ -132,3 +146,21 @@ def get_geometry(txLUT: dict, axLUT: dict, device: torch.device) -> Geometry:
             g._lut_refs = (txLUT['crs'], txLUT['s2c'], axLUT['li2rng'], axLUT['li2sn'],
                            axLUT['li2sn1'], axLUT['li2nos'])
         return g
+
+
+def projector(params: dict, device):
+    """`project(img, span, att)`: the full forward projection [68516, nsinos] (837 at span
+    11, 4084 at span 1; att 1 = attenuation factors) of a [320, 320, 127] image tensor on
+    `device`, by this library's projector (nb_fprj).  The synthetic-data builders take any
+    callable of this form."""
+    dev = torch.device(device)
+    geom = get_geometry(params['txLUT'], params['axLUT'], dev)
+    lib = _lib.load()
+
+    def project(img: torch.Tensor, span: int, att: int) -> torch.Tensor:
+        x = img.to(dev, torch.float32).contiguous()
+        out = torch.empty((geom.naw, 837 if span == 11 else 4084), device=dev)
+        _lib.check(lib.nb_fprj(geom.handle, dev_ptr(out), dev_ptr(x), None, geom.naw, span,
+                               att, stream_ptr(dev)))
+        return out
+    return project

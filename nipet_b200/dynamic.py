@@ -18,8 +18,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import _lib, batch, diffprj, mmrrec, phantoms
-from .device import dev_ptr, get_geometry, stream_ptr
+from . import batch, diffprj, mmrrec, phantoms
 
 __all__ = ['frame_counts', 'dynamic_scan', 'DynamicRecon']
 
@@ -48,7 +47,8 @@ def frame_counts(nframes: int = 16, lo: float = 2e5, hi: float = 5e7, seed: int 
     return counts, t0, dur
 
 
-def dynamic_scan(params: dict, device, counts, seed: int = 0, randoms_frac: float = 0.2):
+def dynamic_scan(params: dict, device, counts, seed: int = 0, randoms_frac: float = 0.2,
+                 project=None):
     """Seeded span-1 dynamic scan on `device`: brain phantom, water attenuation,
     log-normal crystal efficiencies, `randoms_frac` uniform randoms, and Poisson prompts
     for every frame (frame k has counts[k] expected counts).
@@ -56,16 +56,13 @@ def dynamic_scan(params: dict, device, counts, seed: int = 0, randoms_frac: floa
     Returns a dict: `psng` [F, 68516, 4084] uint16 prompts, `an` [68516, 4084] attenuation
     x normalisation, `rs` [68516, 4084] unit randoms / (a n) (0 where a n ~ 0), `rscale`
     [F] each frame's randoms per bin, `counts`, `x_true`, `mu`, `nsng`."""
+    from .device import projector
     dev = torch.device(device)
-    geom = get_geometry(params['txLUT'], params['axLUT'], dev)
-    lib = _lib.load()
-    st = stream_ptr(dev)
+    project = project or projector(params, dev)
     x_true = torch.from_numpy(phantoms.brain_phantom(seed)).to(dev)
     mu = torch.from_numpy(phantoms.water_mumap()).to(dev)
-    asng = torch.empty((NAW, NSN1), device=dev)
-    ex = torch.empty((NAW, NSN1), device=dev)
-    _lib.check(lib.nb_fprj(geom.handle, dev_ptr(asng), dev_ptr(mu), None, NAW, 1, 1, st))
-    _lib.check(lib.nb_fprj(geom.handle, dev_ptr(ex), dev_ptr(x_true), None, NAW, 1, 0, st))
+    asng = project(mu, 1, 1)
+    ex = project(x_true, 1, 0)
     nsng = mmrrec.norm_sinogram_gpu(params, phantoms.crystal_efficiencies(seed), dev, span=1)
     an = (asng * nsng).contiguous()
     del asng
@@ -84,7 +81,6 @@ def dynamic_scan(params: dict, device, counts, seed: int = 0, randoms_frac: floa
         rscale[k] = r
         del mean
     rs = torch.where(an.abs() < 1e-6, torch.zeros_like(an), 1.0 / an)
-    geom.check()
     return {'psng': psng, 'an': an, 'rs': rs, 'rscale': rscale, 'counts': counts,
             'x_true': x_true, 'mu': mu, 'nsng': nsng}
 

@@ -125,6 +125,11 @@ def transaxial_lut(Cnt: dict) -> dict:
     lin = ia + iw * NSA
     c2sF[c1, c0] = lin
     c2sF[c0, c1] = lin
+    # the same with the projection bin changing fastest (used by the scatter model)
+    c2sFw = -np.ones((NCRS, NCRS), dtype=np.int32)
+    linw = iw + ia * NSB
+    c2sFw[c1, c0] = linw
+    c2sFw[c0, c1] = linw
 
     Naw = int(live.sum())
     # live bins, bin-major / angle-minor, exactly the reference's `awi` order
@@ -139,7 +144,8 @@ def transaxial_lut(Cnt: dict) -> dict:
     cij = np.zeros((Cnt['NCRSR'], Cnt['NCRSR']), dtype=np.int8)
     cij[s2cr[:, 0], s2cr[:, 1]] = 1
     cij[s2cr[:, 1], s2cr[:, 0]] = 1
-    return {'crs': crs, 'crsri': crsr, 's2cF': s2cF, 'c2sF': c2sF, 'msino': msino, 'Naw': Naw,
+    return {'crs': crs, 'crsri': crsr, 's2cF': s2cF, 'c2sF': c2sF, 'c2sFw': c2sFw,
+            'msino': msino, 'Naw': Naw,
             's2c': s2c, 's2cr': s2cr, 'cr2s': cr2s, 'aw2sn': aw2sn, 'aw2ali': aw2ali, 'cij': cij}
 
 

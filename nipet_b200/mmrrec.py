@@ -127,19 +127,18 @@ def norm_sinogram_gpu(params: dict, eff: np.ndarray, device, span: int = 11) -> 
 
 
 def synthetic_scan(params: dict, device, seed: int = 0, counts: float = 3e7,
-                   randoms_frac: float = 0.2) -> dict:
+                   randoms_frac: float = 0.2, project=None) -> dict:
     """Seeded synthetic span-11 scan on `device` (float32 / uint16 tensors, gap-free
     [68516, 837] layout): `psng` prompts, `rsng` randoms, `ssng` scatter (0), `nsng` norm,
-    `asng` attenuation factors, plus the truth image `x_true` and its noise-free mean."""
-    geom = get_geometry(params['txLUT'], params['axLUT'], device)
-    lib = _lib.load()
-    st = stream_ptr(device)
+    `asng` attenuation factors, plus the truth image `x_true` and its noise-free mean.
+    `project(img, span, att)` makes the forward projections (default: this library's,
+    `device.projector`)."""
+    from .device import projector
+    project = project or projector(params, device)
     x_true = torch.from_numpy(phantoms.brain_phantom(seed)).to(device)
     mu = torch.from_numpy(phantoms.water_mumap()).to(device)
-    asng = torch.empty((NAW, 837), device=device)
-    ex = torch.empty((NAW, 837), device=device)
-    _lib.check(lib.nb_fprj(geom.handle, dev_ptr(asng), dev_ptr(mu), None, NAW, 11, 1, st))
-    _lib.check(lib.nb_fprj(geom.handle, dev_ptr(ex), dev_ptr(x_true), None, NAW, 11, 0, st))
+    asng = project(mu, 11, 1)
+    ex = project(x_true, 11, 0)
     nsng = norm_sinogram_gpu(params, phantoms.crystal_efficiencies(seed), device)
     trues = asng * nsng * ex
     scale = (1.0 - randoms_frac) * counts / float(trues.double().sum())

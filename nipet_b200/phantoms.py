@@ -94,14 +94,14 @@ def norm_sinogram(params: dict, eff: np.ndarray, span: int = 11) -> np.ndarray:
 # ---------------------------------------------------------------------------------------
 def lm_stream_fast(n_events: int, duration_s: int, params: dict | None = None, seed: int = 0,
                    device='cuda', delayed_frac: float = 0.2, tag_every_ms: int = 1,
-                   t0_ms: int = 1000, weights: str = 'phantom'):
+                   t0_ms: int = 1000, weights: str = 'phantom', project=None):
     """GPU version of `lm_stream` for benchmark-sized streams (returns a device int32
     tensor).  With weights='phantom' prompt addresses are drawn proportional to the
-    attenuated span-1 forward projection of `brain_phantom(seed)`."""
+    attenuated span-1 forward projection of `brain_phantom(seed)`, made by
+    `project(img, span, att)` (default: this library's, `device.projector`)."""
     import torch
 
-    from . import _lib
-    from .device import dev_ptr, get_geometry, stream_ptr
+    from .device import projector
     if params is None:
         from .geometry import get_mmrparams
         params = get_mmrparams()
@@ -112,15 +112,11 @@ def lm_stream_fast(n_events: int, duration_s: int, params: dict | None = None, s
     n_del = int(round(n_events * delayed_frac))
     n_pr = n_events - n_del
     if weights == 'phantom':
-        geom = get_geometry(params['txLUT'], params['axLUT'], dev)
-        lib = _lib.load()
-        st = stream_ptr(dev)
+        project = project or projector(params, dev)
         x = torch.from_numpy(brain_phantom(seed)).to(dev)
         mu = torch.from_numpy(water_mumap()).to(dev)
-        em = torch.empty((68516, 4084), device=dev)
-        at = torch.empty((68516, 4084), device=dev)
-        _lib.check(lib.nb_fprj(geom.handle, dev_ptr(em), dev_ptr(x), None, 68516, 1, 0, st))
-        _lib.check(lib.nb_fprj(geom.handle, dev_ptr(at), dev_ptr(mu), None, 68516, 1, 1, st))
+        em = project(x, 1, 0)
+        at = project(mu, 1, 1)
         w = (em * at).reshape(-1).double()
         del em, at
         cdf = torch.cumsum(w, 0)

@@ -8,6 +8,7 @@
  *   orc_fprj           <- niftypet/nipet/prj/src/prjf.cu:33-206   (fprj_drct, fprj_oblq)
  *   orc_bprj           <- niftypet/nipet/prj/src/prjb.cu:33-187   (bprj_drct, bprj_oblq)
  *   orc_osem_iter      <- niftypet/nipet/prj/src/recon.cu:318-497 (osem, no PSF)
+ *   orc_osem_batch_iter   the same iteration for several images per walk of a LOR
  *   orc_lm_plan        <- niftypet/nipet/lm/src/lmaux.cu:17-270   (getLMinfo, modifyLMinfo)
  *   orc_hist           <- niftypet/nipet/lm/src/hst.cu:37-244     (hst) + lmproc.cu:156-193
  *   orc_philox4x32     <- Philox4x32-10, Salmon et al., SC'11 ("Parallel random numbers:
@@ -604,6 +605,236 @@ void orc_osem_iter(double *img, const unsigned short *psng, const float *rsng, c
   free(imf);
   free(esng);
   free(ratio);
+  free(bimg);
+}
+
+/* ========================================================================
+ * One OSEM iteration over all subsets for B images at once (recon.cu:318-497 applied to
+ * every image, PSF off), as orc_osem_iter does for one: image b has its own prompts
+ * psng[b] and randoms + scatter scaled by rscale[b]; attenuation, normalisation, the
+ * sensitivity images and the mask are shared.  For each LOR of a subset the forward
+ * projection of all its rays (every sum in orc_fprj's order), the ratio y / (Ax + rscale
+ * (r+s)/(an)) with the 1e-6 rules, and the back projection (orc_bprj's terms) are done for
+ * all B images; the back projection is gathered per image column and added to the image
+ * under a per-column lock, so its additions reach a voxel in a different
+ * (double) order than orc_bprj's.
+ * img: [B][NVOX] double in/out.  psng: [B][AW][snno] uint16.  rscale: [B] double.
+ * rsng, ssng, nsng, asng: [AW][snno] float.  subs: [nsub][nprj].  sens: [nsub][NVOX]
+ * double.  msk: [NVOX] uint8.  Span 11 (li2sn, snno 837) or span 1 (li2sn1, 4084).
+ * ====================================================================== */
+#define RBLK 128 /* rays whose forward sums are swept together */
+void orc_osem_batch_iter(double *img, int B, const unsigned short *psng, const double *rscale,
+                         const float *rsng, const float *ssng, const float *nsng,
+                         const float *asng, const int *subs, int nsub, int nprj,
+                         const double *sens, const unsigned char *msk, const float *tt,
+                         const unsigned char *tv, const float *li2rng, const short *li2sn,
+                         int snno) {
+  const size_t nb = (size_t)AW * snno;
+  const int NCOL = SZ_IMX * SZ_IMY;
+  double *rs = malloc(sizeof(double) * nb);
+#pragma omp parallel for schedule(static)
+  for (size_t i = 0; i < nb; i++) {
+    double an = (double)asng[i] * (double)nsng[i];
+    double r = (double)rsng[i] + (ssng ? (double)ssng[i] : 0.0);
+    rs[i] = WITHIN_EPS(an) ? 0.0 : r / an;
+  }
+  float *imf = malloc(sizeof(float) * (size_t)NVOX * B);    /* [NVOX][B] */
+  double *bimg = malloc(sizeof(double) * (size_t)NVOX * B); /* [NVOX][B] */
+#ifdef _OPENMP
+  omp_lock_t *lk = malloc(sizeof(omp_lock_t) * NCOL);
+  for (int c = 0; c < NCOL; c++) omp_init_lock(&lk[c]);
+#endif
+  long long oob = 0;
+  for (int s = 0; s < nsub; s++) {
+    const int *sub = subs + (size_t)s * nprj;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < NVOX; i++)
+      for (int b = 0; b < B; b++) {
+        imf[(size_t)i * B + b] = (float)img[(size_t)b * NVOX + i];
+        bimg[(size_t)i * B + b] = 0.0;
+      }
+#pragma omp parallel reduction(+ : oob)
+    {
+      int *uvs = malloc(sizeof(int) * STEP_CAP);
+      float *tps = malloc(sizeof(float) * STEP_CAP), *tns = malloc(sizeof(float) * STEP_CAP);
+      axial_t *ax = malloc(sizeof(axial_t) * NLI2R);
+      int *w0 = malloc(sizeof(int) * NLI2R), *w1 = malloc(sizeof(int) * NLI2R);
+      float *tz = malloc(sizeof(float) * NLI2R);
+      double *acc = malloc(sizeof(double) * 2 * RBLK * B); /* [ray pair][+/-][B] */
+      double *fwd = malloc(sizeof(double) * snno * B);
+      float *rat = malloc(sizeof(float) * snno * B);
+      double *col = malloc(sizeof(double) * SZ_IMZ * B);
+      float *zf = calloc(B, sizeof(float));
+      double *sink = calloc(B, sizeof(double));
+/* the B values of voxel w of the current column, or zeros (counted) outside [0, 127) */
+#define VOX(w) (((w) >= 0 && (w) < SZ_IMZ) ? c + (size_t)(w) * B : (oob += B, zf))
+/* the B accumulators of voxel w of the current column, or a discarded sink (counted)
+ * outside [0, 127) */
+#define SLOT(w) (((w) >= 0 && (w) < SZ_IMZ) ? col + (size_t)(w) * B : (oob += B, sink))
+#pragma omp for schedule(dynamic, 4)
+      for (int p = 0; p < nprj; p++) {
+        const int ixt = sub[p];
+        const int n = expand_lor(tt, tv, ixt, uvs, tps, tns, STEP_CAP);
+        const float *t = tt + (size_t)N_TT * ixt;
+        for (int ixz = 0; ixz < NRINGS; ixz++)
+          w0[ixz] = zvox((float)((double)li2rng[2 * ixz] + .5 * SZ_RING));
+        for (int ixz = NRINGS; ixz < NLI2R; ixz++) {
+          axial_setup(li2rng, ixz, t[7], t[5], t[6], &ax[ixz]);
+          w0[ixz] = ax[ixz].w;
+          w1[ixz] = ax[ixz].w_;
+          tz[ixz] = ax[ixz].tzc;
+        }
+        /* forward projection of every ray of the LOR, in blocks of RBLK rays: each ray's
+         * sum runs over the steps in order (orc_fprj's sums); the block's accumulators stay
+         * in cache while the steps are swept */
+        memset(fwd, 0, sizeof(double) * snno * B);
+        for (int r0 = 0; r0 < NLI2R; r0 += RBLK) {
+          const int r1 = r0 + RBLK < NLI2R ? r0 + RBLK : NLI2R;
+          memset(acc, 0, sizeof(double) * 2 * RBLK * B);
+          for (int k = 0; k < n; k++) {
+            const float *c = imf + (size_t)uvs[k] * B;
+            const float tn = tns[k], tp = tps[k];
+            const double l = (double)tn - tp;
+            for (int ixz = r0; ixz < r1; ixz++) {
+              double *A0 = acc + (size_t)2 * (ixz - r0) * B, *A1 = A0 + B;
+              if (ixz < NRINGS) {
+                const float *v0 = VOX(w0[ixz]);
+                for (int b = 0; b < B; b++) A0[b] += l * (double)v0[b];
+              } else if ((tn - tz[ixz]) > 0) {
+                const double a = (double)tz[ixz] - tp, bb = (double)tn - tz[ixz];
+                const float *v0 = VOX(w0[ixz]), *v1 = VOX(w1[ixz]);
+                for (int b = 0; b < B; b++) {
+                  A0[b] += a * (double)v0[b];
+                  A1[b] += a * (double)v1[b];
+                }
+                w0[ixz] += ax[ixz].sgnaz;
+                w1[ixz] -= ax[ixz].sgnaz;
+                v0 = VOX(w0[ixz]);
+                v1 = VOX(w1[ixz]);
+                for (int b = 0; b < B; b++) {
+                  A0[b] += bb * (double)v0[b];
+                  A1[b] += bb * (double)v1[b];
+                }
+                tz[ixz] += ax[ixz].dtz;
+              } else {
+                const float *v0 = VOX(w0[ixz]), *v1 = VOX(w1[ixz]);
+                for (int b = 0; b < B; b++) {
+                  A0[b] += l * (double)v0[b];
+                  A1[b] += l * (double)v1[b];
+                }
+              }
+            }
+          }
+          for (int ixz = r0; ixz < r1; ixz++) {
+            const double *A0 = acc + (size_t)2 * (ixz - r0) * B, *A1 = A0 + B;
+            if (ixz < NRINGS) {
+              for (int b = 0; b < B; b++) fwd[(size_t)li2sn[2 * ixz] * B + b] += A0[b];
+            } else {
+              const int o0 = li2sn[2 * ixz], o1 = li2sn[2 * ixz + 1];
+              for (int b = 0; b < B; b++) {
+                fwd[(size_t)o0 * B + b] += A0[b] * ax[ixz].s;
+                fwd[(size_t)o1 * B + b] += A1[b] * ax[ixz].s;
+              }
+            }
+          }
+        }
+        /* ratio, recon.cu:459-470 (sneladd, sneldiv) */
+        for (int j = 0; j < snno; j++) {
+          const size_t g = (size_t)ixt * snno + j;
+          for (int b = 0; b < B; b++) {
+            const double e = fwd[(size_t)j * B + b] + rscale[b] * rs[g];
+            rat[(size_t)j * B + b] =
+                WITHIN_EPS(e) ? 0.0f : (float)((double)psng[(size_t)b * nb + g] / e);
+          }
+        }
+        /* back projection of the ratio (orc_bprj's terms), one image column at a time */
+        for (int ixz = 0; ixz < NRINGS; ixz++)
+          w0[ixz] = zvox((float)((double)li2rng[2 * ixz] + .5 * SZ_RING));
+        for (int ixz = NRINGS; ixz < NLI2R; ixz++) {
+          w0[ixz] = ax[ixz].w;
+          w1[ixz] = ax[ixz].w_;
+          tz[ixz] = ax[ixz].tzc;
+        }
+        for (int k = 0; k < n; k++) {
+          const float tn = tns[k], tp = tps[k];
+          memset(col, 0, sizeof(double) * SZ_IMZ * B);
+          for (int ixz = 0; ixz < NRINGS; ixz++) {
+            const float *bin = rat + (size_t)li2sn[2 * ixz] * B;
+            const double l = (double)tn - tp;
+            double *d0 = SLOT(w0[ixz]);
+            for (int b = 0; b < B; b++) d0[b] += l * (double)bin[b];
+          }
+          for (int ixz = NRINGS; ixz < NLI2R; ixz++) {
+            const float *bin = rat + (size_t)li2sn[2 * ixz] * B;
+            const float *bin_ = rat + (size_t)li2sn[2 * ixz + 1] * B;
+            if ((tn - tz[ixz]) > 0) {
+              const double a = ((double)tz[ixz] - tp) * ax[ixz].s;
+              const double bb = ((double)tn - tz[ixz]) * ax[ixz].s;
+              double *d0 = SLOT(w0[ixz]), *d1 = SLOT(w1[ixz]);
+              for (int b = 0; b < B; b++) {
+                d0[b] += a * (double)bin[b];
+                d1[b] += a * (double)bin_[b];
+              }
+              w0[ixz] += ax[ixz].sgnaz;
+              w1[ixz] -= ax[ixz].sgnaz;
+              d0 = SLOT(w0[ixz]);
+              d1 = SLOT(w1[ixz]);
+              for (int b = 0; b < B; b++) {
+                d0[b] += bb * (double)bin[b];
+                d1[b] += bb * (double)bin_[b];
+              }
+              tz[ixz] += ax[ixz].dtz;
+            } else {
+              const double l = ((double)tn - tp) * ax[ixz].s;
+              double *d0 = SLOT(w0[ixz]), *d1 = SLOT(w1[ixz]);
+              for (int b = 0; b < B; b++) {
+                d0[b] += l * (double)bin[b];
+                d1[b] += l * (double)bin_[b];
+              }
+            }
+          }
+          double *dst = bimg + (size_t)uvs[k] * B;
+#ifdef _OPENMP
+          omp_set_lock(&lk[uvs[k] / SZ_IMZ]);
+#endif
+          for (int i = 0; i < SZ_IMZ * B; i++) dst[i] += col[i];
+#ifdef _OPENMP
+          omp_unset_lock(&lk[uvs[k] / SZ_IMZ]);
+#endif
+        }
+      }
+#undef VOX
+#undef SLOT
+      free(uvs);
+      free(tps);
+      free(tns);
+      free(ax);
+      free(w0);
+      free(w1);
+      free(tz);
+      free(acc);
+      free(fwd);
+      free(rat);
+      free(col);
+      free(zf);
+      free(sink);
+    }
+    const double *sn = sens + (size_t)s * NVOX;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < NVOX; i++)
+      for (int b = 0; b < B; b++) {
+        const double q = WITHIN_EPS(sn[i]) ? 0.0 : bimg[(size_t)i * B + b] / sn[i];
+        double *x = img + (size_t)b * NVOX + i;
+        *x = msk[i] ? *x * q : 0.0;
+      }
+  }
+  g_oob += oob;
+#ifdef _OPENMP
+  for (int c = 0; c < NCOL; c++) omp_destroy_lock(&lk[c]);
+  free(lk);
+#endif
+  free(rs);
+  free(imf);
   free(bimg);
 }
 

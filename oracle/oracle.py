@@ -42,6 +42,8 @@ def lib():
         L.orc_count_reads.restype = C.c_longlong
         L.orc_osem_iter.argtypes = [P, P, P, P, P, P, P, C.c_int, C.c_int, P, P, P, P, P, P,
                                     C.c_int]
+        L.orc_osem_batch_iter.argtypes = [P, C.c_int, P, P, P, P, P, P, P, C.c_int, C.c_int, P,
+                                          P, P, P, P, P, C.c_int]
         L.orc_philox4x32.argtypes = [P, P, P]
         L.orc_poisson_thresholds.argtypes = [C.c_double, P]
         L.orc_lm_plan.argtypes = [P, C.c_int64, C.c_int, C.c_int, C.c_int, P, P, P, P, P, P, P,
@@ -147,6 +149,29 @@ class Oracle:
                             nsub, nprj, _p(sens), _p(msk), _p(self.tt), _p(self.tv),
                             _p(self.li2rng), _p(self.li2sn11), 837)
         return img.reshape(320, 320, 127)
+
+
+    def osem_batch_iter(self, imgs, psng, rscale, rsng, ssng, nsng, asng, subs, sens, msk,
+                        span=11):
+        """One OSEM iteration over every subset for B images at once (`recon.cu:318-497`
+        per image): imgs [B, 320, 320, 127], psng [B, 68516, nsinos] uint16 prompts, image
+        b's randoms + scatter scaled by rscale[b]; float64 images out.  Span 11 or 1."""
+        imgs = np.ascontiguousarray(imgs, dtype=np.float64).reshape(-1, NVOX).copy()
+        nimg = imgs.shape[0]
+        li2sn, snno = self._span(span)
+        psng = np.ascontiguousarray(psng, dtype=np.uint16)
+        assert psng.shape == (nimg, self.naw, snno)
+        rsc = np.ascontiguousarray(np.broadcast_to(np.asarray(rscale, np.float64), (nimg,)))
+        subs = np.ascontiguousarray(subs, dtype=np.int32)
+        nsub, nprj = subs.shape
+        sens = np.ascontiguousarray(sens, dtype=np.float64).reshape(nsub, NVOX)
+        msk = np.ascontiguousarray(msk, dtype=np.uint8).reshape(-1)
+        f32 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+        lib().orc_osem_batch_iter(_p(imgs), nimg, _p(psng), _p(rsc), _p(f32(rsng)),
+                                  _p(f32(ssng)), _p(f32(nsng)), _p(f32(asng)), _p(subs), nsub,
+                                  nprj, _p(sens), _p(msk), _p(self.tt), _p(self.tv),
+                                  _p(self.li2rng), _p(li2sn), snno)
+        return imgs.reshape(nimg, 320, 320, 127)
 
 
 def philox4x32(ctr, key) -> np.ndarray:

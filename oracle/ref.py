@@ -41,8 +41,11 @@ def load():
         lib.ref_randoms.argtypes = [P] * 9 + [I]
         lib.ref_norm.argtypes = [P, P, I] + [P] * 11 + [I]
         lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
+        lib.ref_remgaps.argtypes = [P, P, I, P]
+        lib.ref_putgaps.argtypes = [P, P, P, I, I]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
-                  lib.ref_hist, lib.ref_psf, lib.ref_randoms):
+                  lib.ref_hist, lib.ref_psf, lib.ref_randoms, lib.ref_remgaps,
+                  lib.ref_putgaps):
             f.restype = I
         _lib = lib
     return _lib
@@ -208,3 +211,28 @@ def norm(params, normcomp, buckets, span=11):
                            _p(a['dtnp']), _p(a['bck']), _p(a['rno']), _p(a['s11']),
                            _p(a['nos']), _p(a['aw']), span), 'norm')
     return out
+
+
+def remgaps(params, sino):
+    """The reference's mmraux.remgaps (mmraux.py:1146-1160 -> remove_gaps): Siemens
+    [nsinos, 252, 344] -> gap-free [68516, nsinos], float32 arithmetic, returned in the
+    input's dtype as the reference does."""
+    sino = np.asarray(sino)
+    nsn = sino.shape[0]
+    s32 = np.ascontiguousarray(sino, np.float32).reshape(nsn, -1)
+    aw = np.ascontiguousarray(params['txLUT']['aw2ali'], np.int32)
+    out = np.zeros((NAW, nsn), np.float32)
+    _check(load().ref_remgaps(_p(out), _p(s32), nsn, _p(aw)), 'remgaps')
+    return out.astype(sino.dtype)
+
+
+def putgaps(params, s, span=11, sino_no=0):
+    """The reference's mmraux.putgaps (mmraux.py:1120-1143 -> put_gaps): gap-free
+    [68516, nsinos] -> [nsinos, 252, 344] with zeros in the gaps, in the input's dtype."""
+    s = np.asarray(s)
+    nsn = sino_no if sino_no > 0 else (837 if span == 11 else 4084)
+    s32 = np.ascontiguousarray(s, np.float32)
+    aw = np.ascontiguousarray(params['txLUT']['aw2ali'], np.int32)
+    out = np.zeros((252, 344, nsn), np.float32)
+    _check(load().ref_putgaps(_p(out), _p(s32), _p(aw), int(sino_no), span), 'putgaps')
+    return np.transpose(out, (2, 0, 1)).astype(s.dtype)

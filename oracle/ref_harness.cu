@@ -379,4 +379,27 @@ int ref_norm(float *sino, const float *geo, int ngeo0, const float *cinf, const 
   return (int)e;
 }
 
+// Gap removal by the reference's remove_gaps (src/scanner_0.cu:107-156) as mmr_auxe.rgaps
+// calls it (src/aux_module.cu:389-440): Siemens sino [snno][252*344] float (host) ->
+// gap-free [68516][snno] float (host).
+int ref_remgaps(float *sng, const float *sino, int snno, const int *aw2ali) {
+  Cnst c = make_cnst(11);
+  remove_gaps(sng, const_cast<float *>(sino), snno, const_cast<int *>(aw2ali), c);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return (int)e;
+}
+
+// Gap insertion by the reference's put_gaps (src/scanner_0.cu:169-241) as mmr_auxe.pgaps
+// calls it (src/aux_module.cu:299-387): gap-free [68516][snno] float (host) -> [252*344][snno]
+// float (host, bin-major as put_gaps writes it; mmraux.putgaps transposes it to
+// [snno][252][344]).  sino_no 0 takes snno from the span (837 or 4084), as pgaps does.
+int ref_putgaps(float *sino, const float *sng, const int *aw2ali, int sino_no, int span) {
+  Cnst c = make_cnst(span);
+  put_gaps(sino, const_cast<float *>(sng), const_cast<int *>(aw2ali), sino_no, c);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return (int)e;
+}
+
 }  // extern "C"

@@ -15,7 +15,8 @@ def gold():
     return np.load(GOLD)
 
 
-@pytest.mark.parametrize('key', ['crs', 's2cF', 's2c', 'aw2ali', 'msino', 'crsri'])
+@pytest.mark.parametrize('key', ['crs', 's2cF', 's2c', 'aw2ali', 'msino', 'crsri', 's2cr',
+                                 'aw2sn', 'cij', 'cr2s', 'c2sF', 'c2sFw'])
 def test_transaxial_lut_matches_reference_builder(params, gold, key):
     a = params['txLUT'][key]
     assert a.dtype == gold[key].dtype and np.array_equal(a, gold[key])
@@ -57,6 +58,48 @@ def test_image_layout_round_trip(params):
     dev = geometry.convert2dev(e7, params['Cnt'])
     assert dev.shape == (320, 320, 127)
     assert np.array_equal(geometry.convert2e7(dev, params['Cnt']), e7)
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope='module')
+def img_gold():
+    return np.load(os.path.join(os.path.dirname(__file__), 'golden', 'img_golden.npz'))
+
+
+def test_image_layouts_match_reference_builders(params, img_gold):
+    """convert2dev / convert2e7 (img/mmrimg.py:28-67) on the seeded image the golden
+    generator used: same shape, dtype and bytes as the reference's functions."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_lut_golden import img_input
+    g = img_gold
+    dev = geometry.convert2dev(img_input(), params['Cnt'])
+    assert tuple(dev.shape) == tuple(g['convert2dev_shape'])
+    assert str(dev.dtype) == str(g['convert2dev_dtype'])
+    assert _sha(dev) == str(g['convert2dev_sha256'])
+    back = geometry.convert2e7(np.ascontiguousarray(dev), params['Cnt'])
+    assert tuple(back.shape) == tuple(g['convert2e7_shape'])
+    assert str(back.dtype) == str(g['convert2e7_dtype'])
+    assert _sha(back) == str(g['convert2e7_sha256'])
+
+
+@pytest.mark.parametrize('name,kw', [('cyl29', {'rad': 29., 'xo': 0, 'yo': 0, 'unival': 1}),
+                                     ('cyl25', {}),
+                                     ('cyl_off', {'rad': 12.5, 'xo': 3.0, 'yo': -2.0,
+                                                  'unival': 2.5})])
+def test_cylinder_masks_match_reference_builder(params, img_gold, name, kw):
+    """get_cylinder (img/mmrimg.py:208-227), Siemens and GPU layouts, against the
+    reference's own function: the OSEM mask (29 cm), the default, and an offset one."""
+    cyl = geometry.get_cylinder(params['Cnt'], **kw)
+    assert tuple(cyl.shape) == tuple(img_gold[f'{name}_shape'])
+    assert cyl.dtype == img_gold[f'{name}_slice'].dtype
+    assert all(np.array_equal(cyl[z], img_gold[f'{name}_slice']) for z in range(cyl.shape[0]))
+    cyl_dev = geometry.get_cylinder(params['Cnt'], gpu_dim=True, **kw)
+    assert _sha(cyl_dev) == str(img_gold[f'{name}_dev_sha256'])
 
 
 def test_cylinder_mask(params):

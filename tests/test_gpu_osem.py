@@ -1,6 +1,7 @@
 """GPU parity of the fused OSEM sub-iteration (petprj.osem drop-in) against the FP64
-oracle's restatement of recon.cu:318-497.  Bar: relative L2 error <= 1e-4 of the image,
-after one iteration on small subsets and after 4 x 14 iterations at full size."""
+oracle's restatement of recon.cu:318-497.  Bar: relative L2 error <= 1e-4 of the image
+after one iteration on small subsets (4 x 14 iterations at full size, through the drop-in
+and the batched paths: test_gpu_headline.py)."""
 import numpy as np
 import pytest
 import torch
@@ -70,47 +71,3 @@ def test_osem_torch_inputs_no_host_copy(params, oracle, cuda_device):
     # the image accumulation is a float reduce-add across CTAs, so runs agree to rounding
     got = img_t.cpu().numpy()
     assert np.linalg.norm(got - img_np) <= 1e-6 * np.linalg.norm(img_np)
-
-
-def test_osem_4x14_full_size_matches_oracle(params, oracle, cuda_device):
-    """The bar at full size: a 3e7-count span-11 scan, all 68516 LORs in the 14 subsets
-    the reference uses, 4 iterations, the image against the FP64 oracle's (which runs on
-    the host cores, ~1 min): relative L2 <= 1e-4 inside the mask, through the plain
-    drop-in (`petprj.bprj` sensitivity + `petprj.osem`) and through the batched path."""
-    import os
-    from nipet_b200 import batch, mmrrec
-    from oracle import oracle as O
-    O.set_threads(os.cpu_count() or 1)
-    scan = mmrrec.synthetic_scan(params, cuda_device, seed=4, counts=3e7)
-    h = {k: scan[k].cpu().numpy() for k in ('psng', 'rsng', 'ssng', 'nsng', 'asng')}
-    an = h['asng'] * h['nsng']
-    tab = mmrrec.subset_table(params)
-    subs = tab[:, 1:]
-    msk = geometry.get_cylinder(params['Cnt'], rad=29., xo=0, yo=0, unival=1, gpu_dim=True) > 0.9
-    sens_ref = np.stack([oracle.bprj(an[s], s) for s in subs])
-    ref = np.ones((320, 320, 127), np.float64)
-    for _ in range(4):
-        ref = oracle.osem_iter(ref, h['psng'], h['rsng'], h['ssng'], h['nsng'], h['asng'], subs,
-                               sens_ref, msk)
-    m = msk & (ref > 0)
-
-    sens = np.zeros((14, 320, 320, 127), np.float32)
-    for n in range(14):
-        petprj.bprj(sens[n], an[subs[n]], params['txLUT'], params['axLUT'], subs[n],
-                    params['Cnt'])
-    img = np.ones((320, 320, 127), np.float32)
-    for _ in range(4):
-        petprj.osem(img, h['psng'], h['rsng'], h['ssng'], h['nsng'], h['asng'], tab, sens, msk,
-                    np.full((3, 17), -1, np.float32), params['txLUT'], params['axLUT'],
-                    params['Cnt'])
-    rl2 = np.linalg.norm(img[m] - ref[m]) / np.linalg.norm(ref[m])
-    assert rl2 <= 1e-4, f'drop-in: relative L2 error {rl2:.3e}'
-
-    a = scan['asng'] * scan['nsng']
-    rs = torch.where(a.abs() < 1e-6, torch.zeros_like(a), scan['rsng'] / a)
-    br = batch.BatchRecon(params, scan['psng'].unsqueeze(0), rs, a, device=cuda_device, bs=1)
-    br.run(niter=4)
-    got = br.images()[0].cpu().numpy()
-    br.geom.check()
-    rl2b = np.linalg.norm(got[m] - ref[m]) / np.linalg.norm(ref[m])
-    assert rl2b <= 1e-4, f'batched: relative L2 error {rl2b:.3e}'

@@ -134,3 +134,39 @@ def test_oracle_tables_match_reference_tables(params):
     tt, tv = O.siddon_tables(params['txLUT'])
     assert np.array_equal(tt.view(np.uint32), g['tt'].view(np.uint32))
     assert hashlib.sha256(tv.tobytes()).hexdigest() == str(g['tv_sha256'])
+
+
+@pytest.mark.parametrize('span', [11, 1])
+def test_batched_osem_iteration_equals_single(oracle, params, span):
+    """orc_osem_batch_iter (several images per walk of a LOR, the checker of the batched
+    kernels) equals orc_osem_iter run image by image, to double rounding, with a different
+    randoms level per image.  orc_osem_iter is span 11 only, so at span 1 the batch of B
+    images is checked against the same function run one image at a time."""
+    rng = np.random.default_rng(span)
+    nsn = 837 if span == 11 else 4084
+    subs = np.sort(rng.choice(68516, (2, 48), replace=False), axis=1).astype(np.int32)
+    allsub = subs.reshape(-1)
+    nimg = 3
+    psng = np.zeros((nimg, 68516, nsn), np.uint16)
+    for b in range(nimg):
+        psng[b][allsub] = rng.poisson(2.0 + b, (allsub.size, nsn))
+    rsng = np.full((68516, nsn), 0.05, np.float32)
+    ssng = np.zeros_like(rsng)
+    nsng = np.ones_like(rsng)
+    asng = (0.5 + rng.random((68516, nsn))).astype(np.float32)
+    sens = np.stack([oracle.bprj(asng[s], s, span=span) for s in subs])
+    msk = geometry.get_cylinder(params['Cnt'], rad=29., xo=0, yo=0, unival=1,
+                                gpu_dim=True) > 0.9
+    img0 = np.stack([phantoms.brain_phantom(b) for b in range(nimg)]).astype(np.float64)
+    rsc = np.array([1.0, 0.25, 2.0])
+    got = oracle.osem_batch_iter(img0, psng, rsc, rsng, ssng, nsng, asng, subs, sens, msk,
+                                 span=span)
+    for b in range(nimg):
+        if span == 11:
+            want = oracle.osem_iter(img0[b], psng[b], rsng * rsc[b], ssng, nsng, asng, subs,
+                                    sens, msk)
+        else:
+            want = oracle.osem_batch_iter(img0[b:b + 1], psng[b:b + 1], rsc[b:b + 1], rsng,
+                                          ssng, nsng, asng, subs, sens, msk, span=1)[0]
+        assert np.abs(got[b] - want).max() <= 1e-12 * np.abs(want).max()
+        assert np.linalg.norm(got[b] - img0[b]) > 1e-3 * np.linalg.norm(img0[b])
