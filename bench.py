@@ -791,22 +791,37 @@ def run_hist(args, ws, rank, dev):
                     'scaled by replicates; the launch is bound by L2 atomics on counters '
                     'larger than L2, not by DRAM bandwidth'}
     nev = nwords
-    # e2e: pinned host words -> plan -> device -> every output's sinograms in pinned host
-    # memory (span 11, span 1, the bootstrap replicates)
-    lm_pin = torch.from_numpy(lm_host).pin_memory()
+    # e2e through the file API: the stream written to a list-mode file once (outside the
+    # timing); every step reads the file (`mmr_lmproc.read_stream`: several threads, chunks
+    # moving to the device as they are read), plans, histograms, and copies every output's
+    # prompt/delayed sinograms into pinned host memory on a copy stream, each copy starting
+    # as soon as its histogram is unpacked (the bootstrap replicates, the largest output,
+    # first)
+    td = tempfile.mkdtemp()
+    path = os.path.join(td, 'lm.bf')
+    lm_host.astype('<i4').tofile(path)
+    order = [2, 1, 0]
     outs = {i: (torch.empty((nrep, nbins[C['SPN']]), dtype=torch.uint16).pin_memory(),
                 torch.empty((nrep, nbins[C['SPN']]), dtype=torch.uint16).pin_memory())
             for i, (C, nrep) in enumerate(calls)}
+    cps = torch.cuda.Stream(dev)
 
     def e2e_step():
-        p2 = mmr_lmproc.plan(lm_pin.numpy())
-        for i, (C, nrep) in enumerate(calls):
-            r = mmr_lmproc.hist_stream(lm_pin, params['txLUT'], params['axLUT'], C, pl=p2,
+        lh, d_lm = mmr_lmproc.read_stream(path, Cnt11)
+        p2 = mmr_lmproc.plan(lh)
+        keep = []
+        for i in order:
+            C, nrep = calls[i]
+            r = mmr_lmproc.hist_stream(d_lm, params['txLUT'], params['axLUT'], C, pl=p2,
                                        nrep=nrep, seed=rank + 7)
-            outs[i][0].copy_(r['psn'].reshape(nrep, -1))
-            outs[i][1].copy_(r['dsn'].reshape(nrep, -1))
-            del r
+            cps.wait_stream(torch.cuda.current_stream(dev))
+            with torch.cuda.stream(cps):
+                outs[i][0].copy_(r['psn'].reshape(nrep, -1), non_blocking=True)
+                outs[i][1].copy_(r['dsn'].reshape(nrep, -1), non_blocking=True)
+            keep.append(r)
+        cps.synchronize()
         torch.cuda.synchronize(dev)
+        del keep
 
     e2e_step()
     et = []
@@ -816,10 +831,31 @@ def run_hist(args, ws, rank, dev):
         e2e_step()
         et.append(time.perf_counter() - t)
     te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    # the file API for one span-11 histogram (mmr_lmproc.hist: every output into the
+    # caller's numpy arrays), as a user histograms one frame of a real file
+    dic = {'psn': np.zeros(nbins[11], np.uint16), 'dsn': np.zeros(nbins[11], np.uint16),
+           'ssr': np.zeros(127 * 86688, np.uint32), 'phc': np.zeros(ntag, np.uint32),
+           'dhc': np.zeros(ntag, np.uint32), 'mss': np.zeros(ntag, np.float32),
+           'pvs': np.zeros(mmr_lmproc.sne_for(ntag), np.uint32),
+           'bck': np.zeros(2 * 224 * ntag, np.uint32), 'fan': np.zeros(64 * 504, np.uint32)}
+    mmr_lmproc.hist(dic, path, 0, 0, params['txLUT'], params['axLUT'], Cnt11)
+    ft = []
+    for _ in range(3):
+        t = time.perf_counter()
+        mmr_lmproc.hist(dic, path, 0, 0, params['txLUT'], params['axLUT'], Cnt11)
+        ft.append(time.perf_counter() - t)
+    os.unlink(path)
+    os.rmdir(td)
+    file_span11 = {'value': nev / float(np.mean(ft)), 'unit': 'events/s',
+                   'path': 'mmr_lmproc.hist(dicout, file, ...): read, plan, span-11 histogram, '
+                           'every output into host numpy arrays'}
     res = {'ms_per_step': t_step * 1e3, 'value': ws * nev / t_step,
            'e2e': {'value': ws * nev / te, 'unit': 'events/s', 'h2d_bytes_per_step': nev * 4,
                    'd2h_bytes_per_step': sum(2 * 2 * nrep * nbins[C['SPN']]
-                                             for C, nrep in calls)},
+                                             for C, nrep in calls),
+                   'path': 'list-mode file -> mmr_lmproc.read_stream -> plan -> hist_stream x3 '
+                           '-> prompt/delayed sinograms in pinned host memory',
+                   'file_span11': file_span11},
            'clocks': clocks, 'gpu_launches': sum(1 + nrep for _, nrep in calls),
            'roofline': roof,
            'config': {'workload': f'list-mode histogram of {nev} words over {args.duration} s: '

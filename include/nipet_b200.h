@@ -286,6 +286,30 @@ int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t 
  * memory of calls still in flight on a stream stays until they finish. */
 int nb_hist_trim(void);
 
+/* ---- scatter (sct/src/sct.cu prob_scatt, ray.cu raysLUT, sctaux.cu srslt2sino) ----------
+ * nb_sct_vsm replaces nifty_scatter.vsm (sct/src/sct_module.cu:60-335 -> prob_scatt,
+ * sct.cu:338-582): the voxel-driven single-scatter model for the mMR's 64 scatter crystals
+ * x 8 scatter rings, non-TOF.
+ *   mu     host [63][172][172] float: the down-sampled mu-map (1/cm)
+ *   mumsk  host [63][172][172] int8: attenuating voxels (> 0) for which paths are summed
+ *   em     host [43][114][114] float: the down-sampled emission image
+ *   scrs   host [64][3] float (crystal, x, y cm), srng host [8][2] float (ring, z cm),
+ *   isrng  host [8] int16 scatter rings; knlut host [256][2] float Klein-Nishina LUT;
+ *   cosupsmx cos of the largest scatter angle; ethrld emitting-voxel threshold / maximum;
+ *   xsxu   host [64][64] int8; offseg host [nseg0+1] int16; sctaxR host [4096][4] int32,
+ *   sctaxW host [4096][4] float (axial interpolation); sn1_sn11 host [4084] int16
+ *   sval   dev [8][64][8][64] float, overwritten: the raw results (sct_val)
+ *   s3d    dev [nsn][64][64] float, overwritten: the pre-sinograms, nsn 4096 at span 1
+ *          (sinograms past 4083 zero) or 837 at span 11 (sct_3d)
+ *   nvx    host [2] int, may be NULL: attenuating and emitting voxels used.
+ * Synchronous (the mu-map texture lives for the call). */
+int nb_sct_vsm(const float *mu, const int8_t *mumsk, const float *em, const float *scrs,
+               int nscrs, const float *srng, const int16_t *isrng, int nsrng,
+               const float *knlut, float cosupsmx, float ethrld, const int8_t *xsxu,
+               const int16_t *offseg, int nseg0, const int32_t *sctaxR, const float *sctaxW,
+               int nsn64, const int16_t *sn1_sn11, int nsn1, int span, float *sval, float *s3d,
+               int *nvx, void *stream);
+
 /* ---- host -> device transfer ----------------------------------------------------------
  * nb_copy_h2d replaces the per-call pageable cudaMemcpy of the host arrays petprj.osem,
  * fprj and bprj receive (prj/src/prj_module.cu:613-839 -> recon.cu:334-419, and the
@@ -295,6 +319,11 @@ int nb_hist_trim(void);
  * previous chunk runs.  Returns once `src` has been read entirely (the caller may reuse it);
  * the copies are ordered on `stream`.  Calls on one device are serialised. */
 int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *stream);
+/* nb_copy_d2h: the reverse, for the results petprj.osem and bprj copy back into the caller's
+ * host arrays (prj_module.cu:595-600, :826-832): `bytes` from device memory `src`, after the
+ * work queued on `stream`, into pageable host memory `dst`, the DMA of one chunk overlapping
+ * the host threads' unpacking of the previous.  Returns when `dst` holds the data. */
+int nb_copy_d2h(void *dst, const void *src, size_t bytes, void *stream);
 
 #ifdef __cplusplus
 }

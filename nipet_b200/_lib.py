@@ -68,6 +68,9 @@ SIGNATURES = {
                         P], I),
     'nb_hist_trim': ([], I),
     'nb_copy_h2d': ([P, P, C.c_size_t, P], I),
+    'nb_copy_d2h': ([P, P, C.c_size_t, P], I),
+    'nb_sct_vsm': ([P, P, P, P, I, P, P, I, P, C.c_float, C.c_float, P, P, I, P, P, I, P, I, I,
+                    P, P, P, P], I),
     'nb_osem_subset_span1': ([P, P, P, P, P, P, P, P, I, P, P, P], I),
 }
 

@@ -22,7 +22,7 @@ COMMON = ARCH + ['-lineinfo', '-O3', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcom
 # per-file extra flags: the geometry tables spell out every rounding explicitly
 EXTRA = {'nb_geom.cu': ['-fmad=false']}
 SOURCES = ['nb_capi.cu', 'nb_geom.cu', 'nb_prj.cu', 'nb_batch.cu', 'nb_hist.cu', 'nb_psf.cu',
-           'nb_rnd.cu', 'nb_norm.cu', 'nb_stage.cu']
+           'nb_rnd.cu', 'nb_norm.cu', 'nb_stage.cu', 'nb_sct.cu']
 HEADERS = ['nb_common.cuh', 'nb_internal.cuh', 'nb_axial.cuh', 'nb_project.cuh']
 
 

@@ -1,5 +1,5 @@
-// nb_stage.cu -- host -> device copies of large pageable host arrays through pinned staging
-// buffers, the host CPU copy split over several threads.
+// nb_stage.cu -- copies between large pageable host arrays and device memory through pinned
+// staging buffers, the host CPU copy split over several threads.
 //
 // The drop-in operators take host (numpy) arrays like the reference's petprj, whose
 // osem_rec copies ~1.8 GB of sinograms and sensitivity images from pageable memory on
@@ -11,9 +11,11 @@
 //
 // The staging ring (NB_STAGE_SLOTS pinned buffers of NB_STAGE_CHUNK bytes) is allocated on
 // the first call on a device and kept until the process exits.  Calls on one device are
-// serialised by a mutex.  Like a pageable-source cudaMemcpyAsync, a call returns once the
-// whole source has been read into staging memory (the caller may reuse it at once); the
-// DMAs themselves are ordered on the caller's stream.
+// serialised by a mutex.  Host -> device: like a pageable-source cudaMemcpyAsync, a call
+// returns once the whole source has been read into staging memory (the caller may reuse it
+// at once); the DMAs themselves are ordered on the caller's stream.  Device -> host: the
+// copy is ordered after the stream's earlier work and the call returns when the host array
+// holds the data; while the host threads unpack one chunk the DMA engine fills the next.
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -97,6 +99,44 @@ extern "C" int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *strea
     NB_CUDA(cudaMemcpyAsync(d + off, s.buf[slot], n, cudaMemcpyHostToDevice, cs));
     NB_CUDA(cudaEventRecord(s.done[slot], cs));
     slot = (slot + 1) % NB_STAGE_SLOTS;
+  }
+  return NB_OK;
+}
+
+extern "C" int nb_copy_d2h(void *dst, const void *src, size_t bytes, void *stream) {
+  NB_REQUIRE(bytes == 0 || (dst && src), "nb_copy_d2h: NULL pointer");
+  if (bytes == 0) return NB_OK;
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  NB_REQUIRE(dev >= 0 && dev < 64, "nb_copy_d2h: device index above 63");
+  Stage &s = g_stage[dev];
+  int st = stage_init(s);
+  if (st) return st;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const int nthr = copy_threads();
+  std::lock_guard<std::mutex> lk(s.mu);
+  unsigned char *h = static_cast<unsigned char *>(dst);
+  const unsigned char *d = static_cast<const unsigned char *>(src);
+  const size_t nchunk = (bytes + NB_STAGE_CHUNK - 1) / NB_STAGE_CHUNK;
+  // keep up to NB_STAGE_SLOTS chunks in flight; unpack them in order
+  size_t issued = 0;
+  auto issue = [&](size_t c) -> cudaError_t {
+    const int slot = (int)(c % NB_STAGE_SLOTS);
+    const size_t off = c * NB_STAGE_CHUNK;
+    const size_t n = bytes - off < NB_STAGE_CHUNK ? bytes - off : NB_STAGE_CHUNK;
+    cudaError_t e = cudaEventSynchronize(s.done[slot]);  // an earlier use of the slot
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.buf[slot], d + off, n, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaEventRecord(s.done[slot], cs);
+    return e;
+  };
+  for (; issued < nchunk && issued < NB_STAGE_SLOTS; issued++) NB_CUDA(issue(issued));
+  for (size_t c = 0; c < nchunk; c++) {
+    const int slot = (int)(c % NB_STAGE_SLOTS);
+    const size_t off = c * NB_STAGE_CHUNK;
+    const size_t n = bytes - off < NB_STAGE_CHUNK ? bytes - off : NB_STAGE_CHUNK;
+    NB_CUDA(cudaEventSynchronize(s.done[slot]));
+    par_copy(h + off, s.buf[slot], n, nthr);
+    if (issued < nchunk) NB_CUDA(issue(issued++));
   }
   return NB_OK;
 }

@@ -57,7 +57,27 @@ def get_mmr_constants() -> dict:
         # decay / quantification corrections of osemone
         'ISOTOPE': 'F18', 'DCYCRR': True,
     }
+    Cnt.update(scatter_constants())
     return Cnt
+
+
+def scatter_constants() -> dict:
+    """Constants of the voxel-driven scatter model (`sct/mmrsct.py`).  NIPET takes them from
+    the un-vendored `ninst` package; the grids follow from the model's compiled image sizes
+    (`sct/src/sct.h`: a 63 x 172 x 172 mu-map and a 43 x 114 x 114 emission image, i.e. the
+    zoom factors below applied to the 127 x 344 x 344 Siemens images) and the physics are
+    published values (511 keV photons, the classical electron radius squared, the mMR's
+    non-TOF detectors, its 430 keV lower energy threshold and ~14.5% energy resolution).
+    The remaining values are stand-ins chosen here and used identically by every
+    implementation compared: the 8 scatter rings spread over the 64 rings, the largest
+    scatter angle (cos 0.725) and the emitting-voxel threshold (5% of the maximum)."""
+    return {
+        'SCTSCLMU': [0.499, 0.5, 0.5], 'SCTSCLEM': [0.34, 0.33, 0.33],
+        'SIRNG': [0, 9, 18, 27, 36, 45, 54, 63],
+        'E511': 511.0, 'R02': 7.940787e-26, 'LLD': 430.0, 'ER': 0.145,
+        'COSUPSMX': 0.725, 'NCOS': 256, 'ETHRLD': 0.05,
+        'TOFBINN': 1, 'TOFBINS': 0.0, 'TOFBIND': 0.0, 'ITOFBIND': 0.0,
+    }
 
 
 def nsinos_for(Cnt: dict) -> int:

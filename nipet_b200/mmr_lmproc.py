@@ -3,9 +3,10 @@
 device) and for several bootstrap replicates in one pass.
 
 The reference streams the file through 32 CUDA streams with host callbacks doing the
-file I/O (`hst.cu:280-528`); here the words are read once into pinned memory, copied to
-the device and histogrammed by one kernel launch (`nb_hist`), bit-exact with the
-reference's chunk/thread-slice time attribution (see nipet_b200/csrc/nb_hist.cu).
+file I/O (`hst.cu:280-528`); here the words are read once into pinned memory by several
+threads, each chunk copied to the device as soon as it is read, and histogrammed by one
+kernel launch (`nb_hist`), bit-exact with the reference's chunk/thread-slice time
+attribution (see nipet_b200/csrc/nb_hist.cu).
 """
 from __future__ import annotations
 
@@ -18,7 +19,7 @@ import torch
 from . import _lib
 from .device import dev_ptr, device_of, stream_ptr, to_device
 
-__all__ = ['lminfo', 'hist', 'hist_stream', 'plan', 'NBINS', 'sne_for']
+__all__ = ['lminfo', 'hist', 'hist_stream', 'plan', 'read_stream', 'NBINS', 'sne_for']
 
 NBINS = {1: 354033792, 11: 72557856, 0: 127 * 86688}
 NSINOS = {1: 4084, 11: 837, 0: 127}
@@ -38,6 +39,53 @@ def _read_words(path: str, Cnt: dict | None = None) -> np.ndarray:
         raise NotImplementedError('only 4-byte mMR event words are supported')
     n = (os.path.getsize(path) - off) // 4
     return np.fromfile(path, dtype=np.int32, count=n, offset=off)
+
+
+READ_CHUNK_WORDS = 16 << 20      # 64 MiB per read
+
+
+def read_stream(path: str, Cnt: dict | None = None, device=None, threads: int | None = None):
+    """A list-mode file read once into pinned host memory by several threads, each chunk
+    copied to the device as soon as it is in, on a side stream, so the file read and the
+    host-to-device transfer overlap (the reference overlaps them with 32 streams and
+    host callbacks, `lm/src/hst.cu:280-528`).  Returns (host words [n] int32 numpy view
+    of pinned memory, device words [n] int32 tensor); the device copy is complete on the
+    current stream when this returns."""
+    from concurrent.futures import ThreadPoolExecutor
+    bpe = int(Cnt.get('BPE', 4)) if Cnt else 4
+    off = int(Cnt.get('LMOFF', 0)) if Cnt else 0
+    if bpe != 4:
+        raise NotImplementedError('only 4-byte mMR event words are supported')
+    dev = device_of(Cnt, device)
+    n = (os.path.getsize(path) - off) // 4
+    host = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    d_lm = torch.empty(n, dtype=torch.int32, device=dev)
+    hb = host.numpy().view(np.uint8)
+    chunks = [(a, min(a + READ_CHUNK_WORDS, n)) for a in range(0, n, READ_CHUNK_WORDS)]
+
+    def read(ab):
+        a, b = ab
+        with open(path, 'rb', buffering=0) as f:
+            f.seek(off + 4 * a)
+            mv = memoryview(hb[4 * a:4 * b])
+            got = 0
+            while got < mv.nbytes:
+                k = f.readinto(mv[got:])
+                if not k:
+                    raise IOError(f'{path}: short read at word {a + got // 4}')
+                got += k
+        return ab
+
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    nthr = threads or min(8, os.cpu_count() or 1)
+    with ThreadPoolExecutor(nthr) as ex:
+        for a, b in ex.map(read, chunks):          # in order, as soon as each is read
+            with torch.cuda.stream(side):
+                d_lm[a:b].copy_(host[a:b], non_blocking=True)
+    torch.cuda.current_stream(dev).wait_stream(side)
+    d_lm.record_stream(torch.cuda.current_stream(dev))
+    return host.numpy(), d_lm
 
 
 def lminfo(path: str):
@@ -154,13 +202,16 @@ def hist_stream(lm, txLUT: dict, axLUT: dict, Cnt: dict, t0: int = 0, t1: int = 
 
 def hist(dicout: dict, path: str, t0: int, t1: int, txLUT: dict, axLUT: dict, Cnt: dict):
     """Fill the preallocated numpy arrays of `dicout` (`psn`, `dsn`, `ssr`, `phc`, `dhc`,
-    `mss`, `pvs`, `bck`, `fan`) in place, as `mmr_lmproc.hist` (`lm_module.cu:174-391`)."""
-    lm = _read_words(path, Cnt)
-    r = hist_stream(lm, txLUT, axLUT, Cnt, t0=t0, t1=t1)
+    `mss`, `pvs`, `bck`, `fan`) in place, as `mmr_lmproc.hist` (`lm_module.cu:174-391`).
+    The file is streamed (`read_stream`): read once, into pinned memory, while the chunks
+    already read move to the device."""
+    lm_host, d_lm = read_stream(path, Cnt)
+    r = hist_stream(d_lm, txLUT, axLUT, Cnt, t0=t0, t1=t1, lm_host=lm_host)
+    from .petprj import _writeback
     for k in ('psn', 'dsn', 'ssr', 'phc', 'dhc', 'mss', 'pvs', 'bck', 'fan'):
         dst = dicout[k]
-        src = r[k].cpu().numpy()
-        np.copyto(dst.reshape(-1)[:src.size], src.reshape(-1).astype(dst.dtype, copy=False))
+        src = r[k].reshape(-1)
+        _writeback(dst.reshape(-1)[:src.numel()], src)
 
 
 def trim():

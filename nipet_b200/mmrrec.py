@@ -47,6 +47,7 @@ ISOTOPES = {
 }
 
 RecOut = namedtuple('RecOut', 'im, fpet, imsmo, fsmo, affine')
+RecOutSinos = namedtuple('RecOutSinos', 'im, fpet, imsmo, fsmo, affine, sinos')
 
 
 def fwhm2sig(fwhm, voxsize=1.0):
@@ -267,6 +268,20 @@ class Recon:
                                            st))
         self.launches += 2
 
+    def set_scatter(self, ssng):
+        """Replace the scatter sinogram ([68516, nsinos], gap-free) and recompute
+        (r + s) / (a n) for the following sub-iterations (scatter re-estimated between
+        iterations, `prj/mmrrec.py:363-373`)."""
+        dev = self.device
+        s = torch.as_tensor(np.asarray(ssng, np.float32) if not isinstance(ssng, torch.Tensor)
+                            else ssng).to(dev, torch.float32).contiguous()
+        if tuple(s.shape) != (NAW, self.nsn):
+            raise ValueError(f'ssng must have shape {(NAW, self.nsn)} at span {self.span}')
+        self.ssng = s
+        _lib.check(self.lib.nb_osem_rs(dev_ptr(self.rs), dev_ptr(self.rsng), dev_ptr(self.ssng),
+                                       dev_ptr(self.asng), dev_ptr(self.nsng), NAW * self.nsn,
+                                       stream_ptr(dev)))
+
     def iterate(self, img128: torch.Tensor, niter: int = 1):
         for _ in range(niter):
             for i in range(self.nsub):
@@ -357,9 +372,11 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
     quantification factors, and the Siemens-layout image (Gaussian post-smoothing when
     `fwhm` > 0).  Returns `RecOut(im, fpet, imsmo, fsmo, affine)`.
 
-    Modes: 0 (randoms only), 1 (+ attenuation), 2 (+ the given scatter).  Mode 3 (scatter
-    re-estimated between iterations by `sct/`) and NIfTI output (`store_img`,
-    `store_itr`) are not provided."""
+    Modes: 0 (randoms only), 1 (+ attenuation), 2 (+ the given scatter), 3 and above (+
+    scatter re-estimated by the voxel-driven model, `mmrsct.vsm`, after every iteration but
+    the last, from the current image; `ret_sinos` asks it for its SSRB sinograms and mask,
+    returned as the `RecOut`'s extra `sinos` entry like the reference's `ret_sinos`).
+    NIfTI output (`store_img`, `store_itr`) is not provided."""
     from . import geometry as geo
     from . import mmrhist, mmrnorm
     from scipy import ndimage as ndi
@@ -369,9 +386,6 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
     if span not in (1, 11):
         raise ValueError(f'unrecognised span {span}')
     nsn = 837 if span == 11 else 4084
-    if recmod >= 3:
-        raise NotImplementedError('scatter estimation (sct/) is not provided: use recmod=2 '
-                                  'with sctsino, or recmod 0/1')
     if recmod == 2 and sctsino is None:
         raise ValueError('recmod 2 needs the scatter sinogram (sctsino)')
     if store_img or store_itr:
@@ -395,21 +409,36 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
         asng = attenuation_sino(mus, scanner_params, dev, span)
     # randoms
     if randsino is not None:
+        rsino = randsino
         rsng = _gapfree(randsino, txLUT, Cnt, dev, torch.float32)
     else:
-        rsn, _ = mmrhist.rand_dev(hst['fansums'], txLUT, axLUT, Cnt)
-        rsng = _gapfree(rsn, txLUT, Cnt, dev, torch.float32)
+        rsino, _ = mmrhist.rand_dev(hst['fansums'], txLUT, axLUT, Cnt)
+        rsng = _gapfree(rsino, txLUT, Cnt, dev, torch.float32)
     ssng = _gapfree(sctsino, txLUT, Cnt, dev, torch.float32) if recmod == 2 else None
     rec = Recon(scanner_params, psng, rsng, nsng, asng, ssng, device=dev,
                 mask_radius=mask_radius, krnl=psf_config(psf, Cnt), span=span)
     rec.sensitivity()
     img = rec.init_image()
+    sinos = None
     for k in range(itr):
         rec.iterate(img, 1)
         if float(img.sum()) < 0.1:
             log.warning('it seems there is not enough true data to render reasonable image')
             itr = k
             break
+        if recmod >= 3 and k < itr - 1 and itr > 1:
+            from . import mmrsct
+            rs_host = rsino.cpu().numpy() if isinstance(rsino, torch.Tensor) else rsino
+            sct = mmrsct.vsm(datain, mumaps, geo.convert2e7(rec.image(img), Cnt).cpu().numpy(),
+                             scanner_params, histo=hst, rsino=rs_host, emmsk=emmskS,
+                             return_ssrb=ret_sinos, return_mask=ret_sinos, normcomp=ncmp,
+                             device=dev)
+            # below its threshold the estimate comes back as (zero sinogram, SSRB, mask)
+            ssn = sct['sino'] if isinstance(sct, dict) else (sct[0] if isinstance(sct, tuple)
+                                                             else sct)
+            if isinstance(sct, dict) and ret_sinos:
+                sinos = {k_: v for k_, v in sct.items() if k_ != 'sino'}
+            rec.set_scatter(_gapfree(ssn, txLUT, Cnt, dev, torch.float32))
     rec.geom.check()
     dcycrr, qf, qf_loc = decay_quant_factors(hst, Cnt, ncmp, decay_ref_time)
     im = geo.convert2e7(rec.image(img) * np.float32(dcycrr * qf * qf_loc), Cnt).cpu().numpy()
@@ -426,4 +455,7 @@ def osemone(datain, mumaps, hst, scanner_params, recmod=3, itr=4, fwhm=0., psf=N
     if fwhm > 0:
         im_smo = ndi.gaussian_filter(im, fwhm2sig(fwhm, voxsize=Cnt['SZ_VOXY'] * 10),
                                      mode='mirror')
-    return RecOut(im, fpet, im_smo, fsmo, image_affine(datain, Cnt))
+    out = RecOut(im, fpet, im_smo, fsmo, image_affine(datain, Cnt))
+    if ret_sinos and sinos is not None:
+        out = RecOutSinos(*out, sinos)
+    return out

@@ -14,7 +14,12 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import dev_ptr, device_of, get_geometry, stream_ptr, to_device
+from .device import STAGED_COPY_BYTES, dev_ptr, device_of, get_geometry, stream_ptr, to_device
+
+_TORCH2NP = {torch.float32: np.dtype('float32'), torch.float64: np.dtype('float64'),
+             torch.int32: np.dtype('int32'), torch.int16: np.dtype('int16'),
+             torch.uint16: np.dtype('uint16'), torch.uint8: np.dtype('uint8'),
+             torch.uint32: np.dtype('uint32')}
 
 __all__ = ['tprj', 'fprj', 'bprj', 'osem', 'nsinos_of', 'NLI2R', 'NAW']
 
@@ -51,7 +56,16 @@ def _writeback(dst, src: torch.Tensor):
         if dst.data_ptr() != src.data_ptr():
             dst.copy_(src.reshape(dst.shape))
     elif isinstance(dst, np.ndarray):
-        np.copyto(dst, src.reshape(dst.shape).cpu().numpy().astype(dst.dtype, copy=False))
+        if (dst.flags.c_contiguous and src.is_cuda and src.is_contiguous()
+                and dst.nbytes == src.numel() * src.element_size()
+                and np.dtype(dst.dtype) == _TORCH2NP.get(src.dtype)
+                and dst.nbytes >= STAGED_COPY_BYTES):
+            with torch.cuda.device(src.device):
+                _lib.check(_lib.load().nb_copy_d2h(dst.ctypes.data_as(C.c_void_p),
+                                                   dev_ptr(src), dst.nbytes,
+                                                   stream_ptr(src.device)))
+        else:
+            np.copyto(dst, src.reshape(dst.shape).cpu().numpy().astype(dst.dtype, copy=False))
     elif hasattr(dst, '__cuda_array_interface__'):
         torch.as_tensor(dst, device=src.device).copy_(src.reshape(tuple(dst.shape)))
     else:

@@ -1,5 +1,6 @@
 #!/bin/sh
-# Compile the reference's own CUDA projectors, OSEM, list-mode histogrammer and randoms, normalisation (sources read in place from the
+# Compile the reference's own CUDA projectors, OSEM, list-mode histogrammer, randoms,
+# normalisation and scatter model (sources read in place from the
 # reference tree, nothing copied) with the test-only harness oracle/ref_harness.cu into
 # oracle/_ref/libnipet_ref.so.  Flags follow the reference's Release build (-O3, no fast
 # math), for sm_100a.
@@ -19,8 +20,10 @@ fi
 mkdir -p "$HERE/_ref"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -std=c++14 -Xcompiler -fPIC -shared \
   -DNIPET_CU_THREADS=1024 -I"$REF/include" -I"$REF/prj/src" -I"$REF/lm/src" -I"$REF/src" \
+  -I"$REF/sct/src" \
   "$REF/prj/src/prjf.cu" "$REF/prj/src/prjb.cu" "$REF/prj/src/tprj.cu" \
   "$REF/prj/src/recon.cu" "$REF/lm/src/lmproc.cu" "$REF/lm/src/hst.cu" \
-  "$REF/lm/src/lmaux.cu" "$REF/lm/src/rnd.cu" "$REF/src/scanner_0.cu" "$REF/src/norm.cu" "$HERE/ref_harness.cu" \
+  "$REF/lm/src/lmaux.cu" "$REF/lm/src/rnd.cu" "$REF/src/scanner_0.cu" "$REF/src/norm.cu" \
+  "$REF/sct/src/sct.cu" "$REF/sct/src/sctaux.cu" "$REF/sct/src/ray.cu" "$HERE/ref_harness.cu" \
   -lcurand -o "$HERE/_ref/libnipet_ref.so"
 echo "$HERE/_ref/libnipet_ref.so"

@@ -42,10 +42,11 @@ def load():
         lib.ref_norm.argtypes = [P, P, I] + [P] * 11 + [I]
         lib.ref_hist.argtypes = [C.c_char_p, I, I, I, I, C.c_float] + [P] * 13 + [P, P, P]
         lib.ref_remgaps.argtypes = [P, P, I, P]
+        lib.ref_sct.argtypes = [P, P, P, P, P, P, C.c_float, C.c_float] + [P] * 9 + [I]
         lib.ref_putgaps.argtypes = [P, P, P, I, I]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
                   lib.ref_hist, lib.ref_psf, lib.ref_randoms, lib.ref_remgaps,
-                  lib.ref_putgaps):
+                  lib.ref_putgaps, lib.ref_sct):
             f.restype = I
         _lib = lib
     return _lib
@@ -236,3 +237,28 @@ def putgaps(params, s, span=11, sino_no=0):
     out = np.zeros((252, 344, nsn), np.float32)
     _check(load().ref_putgaps(_p(out), _p(s32), _p(aw), int(sino_no), span), 'putgaps')
     return np.transpose(out, (2, 0, 1)).astype(s.dtype)
+
+
+def sct(params, mu, mumsk, em, sctLUT, span=11):
+    """The reference's scatter model prob_scatt (sct/src/sct.cu:338-582) on host arrays, as
+    nifty_scatter.vsm calls it: mu [63, 172, 172] and its int8 mask, em [43, 114, 114], the
+    tables of mmrsct.get_sctLUT.  Returns (sval [8, 64, 8, 64], s3d [nsn, 64, 64]) float32,
+    nsn 4096 at span 1 and 837 at span 11, and the call's time in ms (host wall clock)."""
+    import time
+    Cnt, ax = params['Cnt'], params['axLUT']
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    a = {'mu': f32(mu), 'msk': np.ascontiguousarray(mumsk, np.int8), 'em': f32(em),
+         'kn': f32(sctLUT['KN']), 'R': np.ascontiguousarray(sctLUT['sctaxR'], np.int32),
+         'W': f32(sctLUT['sctaxW']), 'off': np.ascontiguousarray(sctLUT['offseg'], np.int16),
+         'scrs': f32(sctLUT['scrs']), 'isr': np.ascontiguousarray(sctLUT['sirng'], np.int16),
+         'srng': f32(sctLUT['srng']), 'xsxu': np.ascontiguousarray(sctLUT['xsxu'], np.int8),
+         'rno': np.ascontiguousarray(ax['sn1_rno'], np.int16),
+         's11': np.ascontiguousarray(ax['sn1_sn11'], np.int16)}
+    sval = np.zeros((8, 64, 8, 64), np.float32)
+    s3d = np.zeros((4096 if span == 1 else 837, 64, 64), np.float32)
+    t = time.perf_counter()
+    _check(load().ref_sct(_p(sval), _p(s3d), _p(a['mu']), _p(a['msk']), _p(a['em']), _p(a['kn']),
+                          float(Cnt['COSUPSMX']), float(Cnt['ETHRLD']), _p(a['R']), _p(a['W']),
+                          _p(a['off']), _p(a['scrs']), _p(a['isr']), _p(a['srng']),
+                          _p(a['xsxu']), _p(a['rno']), _p(a['s11']), span), 'sct')
+    return sval, s3d, (time.perf_counter() - t) * 1e3

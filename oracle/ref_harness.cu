@@ -22,6 +22,7 @@
 #include "prjb.h"
 #include "prjf.h"
 #include "recon.h"
+#include "sct.h"
 
 // resolution-modelling routines of prj/src/recon.cu (defined there, not in its header)
 void setConvolutionKernel(float *krnl);
@@ -397,6 +398,55 @@ int ref_remgaps(float *sng, const float *sino, int snno, const int *aw2ali) {
 int ref_putgaps(float *sino, const float *sng, const int *aw2ali, int sino_no, int span) {
   Cnst c = make_cnst(span);
   put_gaps(sino, const_cast<float *>(sng), const_cast<int *>(aw2ali), sino_no, c);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return (int)e;
+}
+
+// The reference's voxel-driven scatter model, prob_scatt (sct/src/sct.cu:338-582: raysLUT,
+// Psct, srslt2sino), called as nifty_scatter.vsm does (sct/src/sct_module.cu:60-335): host
+// mu-map [63][172][172] with its mask, emission image [43][114][114], the scatter LUTs and
+// constants; non-TOF (TOFBINN 1).  Outputs on the host: sval [8][64][8][64] and s3d
+// [nsn][64][64] (nsn 4096 at span 1, 837 at span 11).
+int ref_sct(float *sval, float *s3d, float *mu, int8_t *mumsk, float *em, float *knlut,
+            float cosupsmx, float ethrld, int *sctaxR, float *sctaxW, int16_t *offseg,
+            float *scrs, int16_t *isrng, float *srng, int8_t *xsxu, int16_t *sn1_rno,
+            int16_t *sn1_sn11, int span) {
+  Cnst c = make_cnst(span);
+  c.NSN64 = NRINGS * NRINGS;
+  c.NSEG0 = SEG0;
+  c.NSCRS = 64;
+  c.NSRNG = 8;
+  c.TOFBINN = 1;
+  c.TOFBINS = 0.f;
+  c.TOFBIND = 0.f;
+  c.ITOFBIND = 0.f;
+  c.COSUPSMX = cosupsmx;
+  c.ETHRLD = ethrld;
+  // image statistics as sct_module.cu:277-306 computes them
+  auto stats = [](float *im, size_t n) {
+    IMflt r;
+    r.im = im;
+    r.nvx = n;
+    float mx = -1e12f, mn = 1e12f;
+    for (size_t i = 0; i < n; i++) {
+      if (im[i] > mx) mx = im[i];
+      if (im[i] < mn) mn = im[i];
+    }
+    r.max = mx;
+    r.min = mn;
+    r.n10mx = 0;
+    for (size_t i = 0; i < n; i++)
+      if (im[i] > 0.1 * mx) r.n10mx += 1;
+    return r;
+  };
+  IMflt muI = stats(mu, (size_t)SS_IMX * SS_IMY * SS_IMZ);
+  IMflt emI = stats(em, (size_t)SSE_IMX * SSE_IMY * SSE_IMZ);
+  scatOUT o;
+  o.sval = sval;
+  o.s3d = s3d;
+  prob_scatt(o, knlut, reinterpret_cast<char *>(mumsk), muI, emI, sctaxR, sctaxW, offseg, scrs,
+             isrng, srng, reinterpret_cast<char *>(xsxu), sn1_rno, sn1_sn11, c);
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaGetLastError();
   return (int)e;

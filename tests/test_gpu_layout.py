@@ -9,8 +9,9 @@ own CUDA build (compiled from its sources into oracle/_ref):
   steps composed from the reference's routines: Siemens (E7) and device image layouts,
   subsets with and without `fullsino_out`, `dev_out` both ways, attenuation, and 3-D
   Siemens sinograms into the back projector.  Projections within 1e-5 per bin (bins
-  above 1e-3 of the maximum), back projections within 1e-5 relative L2, layouts and
-  zero bins exact.
+  above 1e-3 of the maximum; where ours and the reference disagree the FP64 oracle
+  decides, see _arbitrate), back projections within 1e-5 relative L2 of the FP64 oracle,
+  layouts and zero bins exact.
 """
 import os
 import sys
@@ -109,8 +110,42 @@ def test_frwd_prj_matches_reference_composition(params, cuda_device, span, att, 
                      dev_out)
     assert isinstance(got, np.ndarray) and got.shape == want.shape
     assert np.array_equal(got == 0, want == 0), 'zero bins (gaps, rows outside the subset)'
-    rel = _rel_bins(got, want)
-    assert rel <= 1e-5, f'max relative error {rel:.3e}'
+    _arbitrate(params, got, want, ims, isub, span, int(att), dev_out, fullsino_out)
+
+
+# Bins where ours and the reference disagree are settled by the FP64 oracle.  The mMR
+# geometry has one ray -- LOR 42285, rings 31 -> 52 -- whose attenuation line integral the
+# reference's CUDA build returns as 0 (factor exp(0) = 1) for the water mu-map, while its
+# algorithm restated in float64 and this package both give 0.98998 (the ray starts 8e-7 cm
+# below a z plane); the bins that ray feeds (one span-1, one span-11 sinogram) are the only
+# ones the reference gets wrong here.
+MAX_ARBITRATED = 4
+
+
+def _arbitrate(params, got, want, ims, isub, span, att, dev_out, fullsino_out, tol=1e-5):
+    g, w = np.asarray(got, np.float64), np.asarray(want, np.float64)
+    big = np.abs(w) >= 1e-3 * np.abs(w).max()
+    err = np.where(big | (g != w), np.abs(g - w) / np.maximum(np.abs(w), 1e-3 * np.abs(w).max()),
+                   0.0)
+    bad = np.argwhere(err > tol)
+    assert len(bad) <= MAX_ARBITRATED, f'{len(bad)} bins differ from the reference (max ' \
+                                       f'{err.max():.3e})'
+    if not len(bad):
+        return
+    from oracle import oracle as O
+    orc = O.Oracle(params)
+    aw = np.asarray(params['txLUT']['aw2ali'], np.int64)
+    for idx in map(tuple, bad):
+        if g.ndim == 3:        # Siemens (sinogram, angle, bin)
+            sn, lor = idx[0], int(np.flatnonzero(aw == idx[2] + 344 * idx[1])[0])
+        else:                  # gap-free (row, sinogram)
+            sn = idx[1]
+            lor = int(isub[idx[0]]) if (isub[0] >= 0 and not fullsino_out) else idx[0]
+        o = orc.fprj(np.ascontiguousarray(ims, np.float32), np.array([lor], np.int32), att=att,
+                     span=span)[0][sn]
+        assert abs(g[idx] - o) <= tol * max(abs(o), 1e-3 * np.abs(w).max()), \
+            f'bin {idx} (LOR {lor}): ours {g[idx]:.7g}, reference {w[idx]:.7g}, FP64 {o:.7g}'
+        assert abs(w[idx] - o) > abs(g[idx] - o), f'bin {idx}: the reference is closer to FP64'
 
 
 @pytest.mark.parametrize('span,siemens,use_sub,dev_out', [
@@ -136,8 +171,18 @@ def test_back_prj_matches_reference_composition(params, cuda_device, span, sieme
     if not dev_out:
         want = geometry.convert2e7(want, Cnt)
     assert got.shape == want.shape == ((320, 320, 127) if dev_out else (127, 344, 344))
-    rl2 = np.linalg.norm(got.astype(np.float64) - want) / np.linalg.norm(want)
-    assert rl2 <= 1e-5, f'relative L2 {rl2:.3e}'
+    # both accumulate float terms in different orders (the reference with float atomics):
+    # the FP64 oracle is the bar (1e-5), and the distance to the reference is bounded by
+    # 1e-5 plus the reference's own distance from the oracle
+    from oracle import oracle as O
+    o = O.Oracle(params).bprj(sinog, None if isub[0] < 0 else isub, span=span)
+    if not dev_out:
+        o = geometry.convert2e7(o, Cnt)
+    rl2 = lambda a, b: np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b)  # noqa: E731
+    e_o, e_r, e_ro = rl2(got, o), rl2(got, want), rl2(want, o)
+    what = f'to FP64 {e_o:.3e}, to the reference {e_r:.3e} (reference to FP64 {e_ro:.3e})'
+    assert e_o <= 1e-5, what
+    assert e_r <= 1e-5 + e_ro, what
 
 
 def test_trnx_prj_matches_reference_tables(params, cuda_device):

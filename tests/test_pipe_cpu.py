@@ -64,8 +64,6 @@ def test_image_affine(params):
 def test_osemone_and_mmrchain_argument_checks(params):
     hst = {'psino': np.zeros((837, 252, 344), np.uint16)}
     mu = [np.zeros((127, 344, 344), np.float32)] * 2
-    with pytest.raises(NotImplementedError, match='scatter'):
-        mmrrec.osemone({}, mu, hst, params, recmod=3)
     with pytest.raises(ValueError, match='sctsino'):
         mmrrec.osemone({}, mu, hst, params, recmod=2)
     with pytest.raises(NotImplementedError, match='NIfTI'):
