@@ -18,6 +18,8 @@ launches 15, 16, 17 are one warm launch of each mode:
 `hist200boot` histograms that stream with 4 Poisson bootstrap replicates per launch (about
 3.4 GB on the device).
 
+`sct` runs the scatter model twice (capture -k regex:k_sct_psct -s 1 -c 1).
+
 `batch` runs one batched OSEM sub-iteration (subset 0) for 8 images with batch widths 4 and
 2, twice each (capture -k regex:k_osem_batch -s 2 -c 2 for the second launch of each width:
 launches 0, 1 are width 4, 2, 3 width 2 -- use -s 1 -c 1 and -s 3 -c 1).
@@ -105,8 +107,28 @@ def batch(device='cuda:0'):
     print('batch ok')
 
 
+def sct(device='cuda:0'):
+    """The scatter model (`nb_sct_vsm`) twice on the brain phantom / water mu-map inputs of
+    the scatter tests (a few hundred MB on the device); launches per call: k_sct_rays,
+    k_sct_psct, k_sct2sn1, k_sct_ax11 -- capture -k regex:k_sct_psct -s 1 -c 1 for the
+    second call's scatter kernel."""
+    import numpy as np
+    from nipet_b200 import geometry, mmrsct, phantoms
+    dev = torch.device(device)
+    p = geometry.get_mmrparams()
+    Cnt = p['Cnt']
+    muo = geometry.convert2e7(phantoms.water_mumap(), Cnt)
+    em = geometry.convert2e7(phantoms.brain_phantom(2), Cnt)
+    mu, msk, emi = mmrsct._zoom_and_smooth(muo, np.zeros_like(muo), em, Cnt, 0.42)
+    lut = mmrsct.get_sctLUT(p)
+    for _ in range(2):
+        mmrsct.scatter_presino(mu, msk, emi, lut, p, device=dev)
+    torch.cuda.synchronize(dev)
+    print('sct ok')
+
+
 if __name__ == '__main__':
-    {'projectors': projectors, 'hist': hist, 'batch': batch,
+    {'projectors': projectors, 'hist': hist, 'batch': batch, 'sct': sct,
      'hist200': lambda: hist(nwords=200_000_000, duration=600),
      'hist200boot': lambda: hist(nwords=200_000_000, duration=600, nrep=4)}[
         sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
