@@ -461,7 +461,7 @@ def run_batch(args, ws, rank, dev):
                               host_an.to(dev, non_blocking=True), rscale=rscale, device=dev,
                               bs=br.bs, tile=br.tile)
         r2.run(niter=4, use_graph=False)
-        m, s = r2.mean_std()
+        m, s = r2.mean_std(distributed=ws > 1)
         m, s = m.cpu(), s.cpu()
         torch.cuda.synchronize(dev)
         et.append(time.perf_counter() - t)
@@ -779,6 +779,8 @@ def run_hist(args, ws, rank, dev):
     p_upd = 1.0 - float(np.exp(-CntB['BTPRT']))
     byt = 4 * nwords + nboot * (8 * (nwords - ntag) * p_upd + 4 * nbins[11])
     dur = float(np.mean([a.elapsed_time(b) for i, a, b in ev if i == ib])) / 1e3
+    call_ms = {name: float(np.mean([a.elapsed_time(b) for i, a, b in ev if i == k]))
+               for k, name in enumerate(('span11', 'span1', f'bootstrap{nboot}'))}
     achieved = byt / dur / 1e9
     peak, peak_kind = _peaks()
     tr = _traffic('hist_200M_boot4')
@@ -786,7 +788,7 @@ def run_hist(args, ws, rank, dev):
             'frac': achieved / peak, 'peak_kind': peak_kind,
             'traffic': None if tr is None else tr * nwords / 200_600_000 * nboot / 4,
             'kernel': f'k_hist, {nboot} Poisson bootstrap replicates at span 11 (one launch)',
-            'launch_ms_avg': dur * 1e3, 'bytes_per_launch': byt,
+            'launch_ms_avg': dur * 1e3, 'bytes_per_launch': byt, 'call_ms': call_ms,
             'note': 'traffic: ncu DRAM bytes of the 4-replicate launch on the same stream, '
                     'scaled by replicates; the launch is bound by L2 atomics on counters '
                     'larger than L2, not by DRAM bandwidth'}

@@ -146,8 +146,13 @@ class BatchRecon:
                                           stream_ptr(self.device)))
         return out
 
-    def mean_std(self):
-        """Voxel-wise mean and standard deviation (ddof=1) over the images."""
+    def mean_std(self, distributed: bool = False, group=None):
+        """Voxel-wise mean and standard deviation (ddof=1) over the images; with
+        `distributed`, over the images of every rank of the process group (each rank
+        reconstructing its own share of one bootstrap set, `shard.replicate_range`)."""
+        if distributed:
+            from .shard import mean_std_over_ranks
+            return mean_std_over_ranks(self.images(), group)
         x = self.images().double()
         return x.mean(0).float(), x.std(0, unbiased=self.nrep > 1).float()
 

@@ -32,3 +32,30 @@ def sum_over_ranks(t):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t)
     return t
+
+
+def mean_std_over_ranks(local, group=None):
+    """Voxel-wise mean and standard deviation (ddof 1) of the images of all ranks: `local`
+    [n_local, ...] holds this rank's replicates (n_local may differ between ranks, and may
+    be 0).  Two all-reduces in float64 -- the sum, then the sum of squared deviations from
+    the global mean (the centred form, which keeps its precision when the spread is small
+    against the mean).  Returns (mean, std) as float32 tensors on `local`'s device; with
+    no process group, the statistics of `local` itself."""
+    import torch
+    import torch.distributed as dist
+    x = local.double()
+    dist_on = dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1
+    n = torch.tensor([float(x.shape[0])], dtype=torch.float64, device=x.device)
+    s1 = x.sum(0)
+    if dist_on:
+        dist.all_reduce(n, group=group)
+        dist.all_reduce(s1, group=group)
+    ntot = float(n.item())
+    if ntot < 1:
+        raise ValueError('no replicates on any rank')
+    mean = s1 / ntot
+    s2 = ((x - mean) ** 2).sum(0)
+    if dist_on:
+        dist.all_reduce(s2, group=group)
+    std = (s2 / (ntot - 1)).sqrt() if ntot > 1 else torch.zeros_like(mean)
+    return mean.float(), std.float()
