@@ -75,6 +75,32 @@ int nb_fprj(nb_geom *g, float *sino, const float *im, const int32_t *subs, int n
 int nb_bprj(nb_geom *g, float *im, const float *sino, const int32_t *subs, int nprj, int span,
             void *stream);
 
+/* ---- span-1 projectors over a reduced axial ring range ---------------------------------
+ * The reference's reduced-rings mode (Cnt.RNG_STRT = rs, Cnt.RNG_END = re, set by
+ * mmraux.reduce_rings, mmraux.py:566-617): petprj.fprj / petprj.bprj in span 1 with the
+ * range's axial LUTs run gpu_fprj / gpu_bprj over the ring pairs inside [rs, re) only, on
+ * an image of the axial slab [2 rs, 2 re - 1) (prj/src/prjf.cu:19-29 imExpand, :209-320;
+ * prjb.cu:19-29 imReduce, :190-308).
+ * nb_rings_create builds the range's ray set once from the range's LUTs:
+ *   li2rng host [nli2r][2] float  (reduced axLUT['li2rng'])
+ *   li2sn1 host [nli2r][2] int16  (reduced axLUT['li2sn1'])
+ *   nli2r  (re-rs)(re-rs+1)/2, less 6 for all 64 rings
+ * Every pair must be a ray of the geometry with both rings in the range, and the rays
+ * must fill the range's nsino = (re-rs)^2 sinograms (4084 for 64 rings) once each.
+ * nb_rings_info: nsino, the slab's first voxel vz0 = 2 rs and its size nvz = 2 (re-rs) - 1.
+ * nb_fprj_rings: sino dev [nprj][nsino] float, overwritten; im dev [320*320*nvz] float.
+ * nb_bprj_rings: im dev [320*320*nvz] float, overwritten; sino dev [nprj][nsino] float.
+ * subs, nprj, att as for nb_fprj. */
+typedef struct nb_rings nb_rings;
+int nb_rings_create(nb_geom *g, int rs, int re, const float *li2rng, const int16_t *li2sn1,
+                    int nli2r, nb_rings **out);
+int nb_rings_destroy(nb_rings *rr);
+int nb_rings_info(const nb_rings *rr, int *nsino, int *vz0, int *nvz);
+int nb_fprj_rings(nb_geom *g, const nb_rings *rr, float *sino, const float *im,
+                  const int32_t *subs, int nprj, int att, void *stream);
+int nb_bprj_rings(nb_geom *g, const nb_rings *rr, float *im, const float *sino,
+                  const int32_t *subs, int nprj, void *stream);
+
 /* ---- the same projectors on the internal "col128" layout -------------------------------
  * col128: nimg images of [320*320][128] float, column-major in z with even z in slots
  * [0,64), odd z in [64,127) and slot 127 zero.  nb_bprj_col128 ADDS into im128.

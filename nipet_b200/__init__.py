@@ -7,9 +7,12 @@ The CUDA kernels and their C ABI live in `libnipet_b200.so` (`csrc/`, built in-t
   `frwd_prj` / `back_prj` operators;
 * `mmr_lmproc`, `mmrhist`: list-mode information, histogramming (with bootstrap) and
   randoms from the delayed fan sums;
-* `mmraux`, `geometry`: sinogram gap conversion, scanner constants and look-up tables;
+* `mmraux`, `geometry`: sinogram gap conversion, scanner constants and look-up tables,
+  and the reduced axial FOV (`reduce_rings`) the projectors also run in;
 * `mmrnorm`: the normalisation sinogram from its components;
 * `mmrrec`, `pipe`: OSEM on device-resident data, `osemone` and `mmrchain`;
+* `mmrsct`: the voxel-driven scatter model and its estimate;
+* `mmrsim`: sinogram simulation and reconstruction of simulated data;
 * `batch`, `dynamic`, `diffprj`: batched bootstrap / dynamic-frame OSEM, the
   differentiable projector (autograd), and the batch-shape autotuner.
 

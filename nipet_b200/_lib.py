@@ -37,6 +37,11 @@ SIGNATURES = {
     'nb_geom_count_reads': ([P, P, C.POINTER(C.c_longlong)], I),
     'nb_fprj': ([P, P, P, P, I, I, I, P], I),
     'nb_bprj': ([P, P, P, P, I, I, P], I),
+    'nb_rings_create': ([P, I, I, P, P, I, C.POINTER(P)], I),
+    'nb_rings_destroy': ([P], I),
+    'nb_rings_info': ([P, C.POINTER(I), C.POINTER(I), C.POINTER(I)], I),
+    'nb_fprj_rings': ([P, P, P, P, P, I, I, P], I),
+    'nb_bprj_rings': ([P, P, P, P, P, I, P], I),
     'nb_fprj_col128': ([P, P, P, P, I, I, I, P], I),
     'nb_bprj_col128': ([P, P, P, P, I, I, P], I),
     'nb_sens_col128': ([P, P, P, P, I, I, P], I),

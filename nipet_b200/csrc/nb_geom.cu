@@ -9,7 +9,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "nb_axial.cuh"
@@ -223,6 +225,7 @@ static void nb_geom_free(nb_geom *g) {
   cudaFree(g->d_err);
   cudaFree(g->d_one);
   free(g->h_s2c);
+  free(g->h_rays);
   free(g);
 }
 
@@ -382,6 +385,13 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
 
   int st = NB_OK;
   unsigned char *d_tv = nullptr;
+  g->h_rays = (nb_ray *)malloc(sizeof(nb_ray) * NB_NRAYS);
+  if (!g->h_rays) {
+    free(g->h_s2c);
+    free(g);
+    return NB_ERR_NOMEM;
+  }
+  memcpy(g->h_rays, rays.data(), sizeof(nb_ray) * NB_NRAYS);
 #define ALLOC(p, bytes)                                                                        \
   do {                                                                                         \
     if (cudaMalloc((void **)&(p), (bytes)) != cudaSuccess) {                                   \
@@ -486,6 +496,136 @@ fail:
   cudaFree(d_tv);
   nb_geom_free(g);
   return st;
+}
+
+// Ring of a ring front edge z (cm): ring i starts at (i - 32) * AXR (mmraux.py:365-370)
+static int ring_of(float z) {
+  const double r = (double)z / (double)NB_RING + 0.5 * NB_NRINGS;
+  const long i = lrint(r);
+  return fabs(r - (double)i) < 1e-4 ? (int)i : -1;
+}
+
+// Rays of the ring range [rs, re) from the range's axial LUTs, as mmraux.axial_lut builds
+// them after mmraux.reduce_rings: li2rng / li2sn1 [nli2r][2], the first re - rs entries
+// the direct planes (prjf.cu:33-95 runs them as fprj_drct), the others the oblique pairs,
+// whose ring r0 -> r1 ray feeds sinogram li2sn1[.][0] and r1 -> r0 li2sn1[.][1]
+// (prjf.cu:98-206).  Each ray must be one of the geometry's rays with both rings in the
+// range, and the rays must fill the range's (re - rs)^2 sinograms (4084 for all 64 rings)
+// once each; anything else is NB_ERR_ARG (the reference's LUTs of 62- and 63-ring ranges,
+// whose ring differences exceed the maximum of 60 without the full-ring correction, end in
+// zero entries and fail this check).  The rays keep the geometry's warp-friendly order.
+extern "C" int nb_rings_create(nb_geom *g, int rs, int re, const float *li2rng,
+                               const int16_t *li2sn1, int nli2r, nb_rings **out) {
+  NB_REQUIRE(out != nullptr, "nb_rings_create: out is NULL");
+  *out = nullptr;
+  NB_REQUIRE(g && li2rng && li2sn1, "nb_rings_create: NULL argument");
+  NB_REQUIRE(g->h_rays != nullptr, "nb_rings_create: geometry without a ray table");
+  NB_REQUIRE(rs >= 0 && rs < re && re <= NB_NRINGS, "nb_rings_create: need 0 <= rs < re <= 64");
+  const int n = re - rs;
+  const int want_li = n * (n + 1) / 2 - (n == NB_NRINGS ? 6 : 0);
+  const int nsino = n * n - (n == NB_NRINGS ? 12 : 0);
+  if (nli2r != want_li) {
+    nb_set_error_msg("nb_rings_create: %d ring pairs given, the range [%d, %d) has %d", nli2r,
+                     rs, re, want_li);
+    return NB_ERR_ARG;
+  }
+  // the geometry's rays by (kind, ring front edges)
+  std::map<std::tuple<int, uint32_t, uint32_t>, int> pos;
+  for (int r = 0; r < NB_NRAYS; r++) {
+    const nb_ray &R = g->h_rays[r];
+    uint32_t a, b;
+    memcpy(&a, &R.r0z, 4);
+    memcpy(&b, &R.r1z, 4);
+    pos[std::make_tuple((int)R.kind, a, b)] = r;
+  }
+  std::vector<std::pair<int, nb_ray>> sel;  // (position in the geometry's order, ray)
+  sel.reserve(nsino);
+  for (int li = 0; li < nli2r; li++) {
+    const float z0 = li2rng[2 * li], z1 = li2rng[2 * li + 1];
+    const int r0 = ring_of(z0), r1 = ring_of(z1);
+    if (r0 < rs || r0 >= re || r1 < rs || r1 >= re) {
+      nb_set_error_msg("nb_rings_create: ring pair %d (z %g, %g cm) is outside rings [%d, %d)",
+                       li, (double)z0, (double)z1, rs, re);
+      return NB_ERR_ARG;
+    }
+    const int nk = li < n ? 1 : 2;
+    for (int k = 0; k < nk; k++) {
+      const int kind = li < n ? 0 : 1 + k;
+      uint32_t a, b;
+      memcpy(&a, &z0, 4);
+      memcpy(&b, &z1, 4);
+      auto it = pos.find(std::make_tuple(kind, a, b));
+      if (it == pos.end()) {
+        nb_set_error_msg("nb_rings_create: ring pair %d (rings %d, %d) is not a %s ray of the "
+                         "geometry", li, r0, r1, kind == 0 ? "direct" : "oblique");
+        return NB_ERR_ARG;
+      }
+      nb_ray R = g->h_rays[it->second];
+      R.out1 = li2sn1[2 * li + k];
+      R.out11 = 0;  // span 11 does not exist for a reduced range
+      sel.emplace_back(it->second, R);
+    }
+  }
+  if ((int)sel.size() != nsino) {
+    nb_set_error_msg("nb_rings_create: %zu rays for %d sinograms", sel.size(), nsino);
+    return NB_ERR_ARG;
+  }
+  std::sort(sel.begin(), sel.end(),
+            [](const std::pair<int, nb_ray> &x, const std::pair<int, nb_ray> &y) {
+              return x.first < y.first;
+            });
+  std::vector<nb_ray> rays(nsino);
+  std::vector<int16_t> bin1(nsino, -1);
+  for (int r = 0; r < nsino; r++) {
+    rays[r] = sel[r].second;
+    const int o = rays[r].out1;
+    if (o < 0 || o >= nsino || bin1[o] != -1) {
+      nb_set_error_msg("nb_rings_create: sinogram %d of the range is out of [0, %d) or mapped "
+                       "twice", o, nsino);
+      return NB_ERR_ARG;
+    }
+    bin1[o] = (int16_t)r;
+  }
+  NB_CUDA(cudaSetDevice(g->device));
+  nb_rings *rr = (nb_rings *)calloc(1, sizeof(nb_rings));
+  if (!rr) return NB_ERR_NOMEM;
+  rr->device = g->device;
+  rr->rs = rs;
+  rr->re = re;
+  rr->nrays = nsino;
+  rr->vz0 = 2 * rs;
+  rr->nvz = 2 * n - 1;
+  cudaError_t e = cudaMalloc(&rr->d_rays, sizeof(nb_ray) * nsino);
+  if (e == cudaSuccess) e = cudaMalloc(&rr->d_bin1, sizeof(int16_t) * nsino);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(rr->d_rays, rays.data(), sizeof(nb_ray) * nsino, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(rr->d_bin1, bin1.data(), sizeof(int16_t) * nsino, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(rr->d_rays);
+    cudaFree(rr->d_bin1);
+    free(rr);
+    return nb_cuda_fail(e, "nb_rings_create upload", __FILE__, __LINE__);
+  }
+  *out = rr;
+  return NB_OK;
+}
+
+extern "C" int nb_rings_destroy(nb_rings *rr) {
+  if (!rr) return NB_OK;
+  cudaSetDevice(rr->device);
+  cudaFree(rr->d_rays);
+  cudaFree(rr->d_bin1);
+  free(rr);
+  return NB_OK;
+}
+
+extern "C" int nb_rings_info(const nb_rings *rr, int *nsino, int *vz0, int *nvz) {
+  NB_REQUIRE(rr != nullptr, "nb_rings_info: NULL handle");
+  if (nsino) *nsino = rr->nrays;
+  if (vz0) *vz0 = rr->vz0;
+  if (nvz) *nvz = rr->nvz;
+  return NB_OK;
 }
 
 extern "C" int nb_geom_destroy(nb_geom *g) {

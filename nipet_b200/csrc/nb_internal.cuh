@@ -38,9 +38,25 @@ struct nb_geom {
   int fxbits;            // fixed-point headroom of the backward accumulators
   int *d_err;            // device error flag
   float *d_one;          // the constant 1.0f (randoms factor of a single-image batch)
-  // host copies of the LUTs (for nb_geom_tables)
+  // host copies of the LUTs (for nb_geom_tables) and of the ray table (for nb_rings_create)
   float h_crs[504 * 4];
   int16_t *h_s2c;
+  nb_ray *h_rays;    // [4084], the order of d_rays
+};
+
+// The rays of a reduced axial ring range [rs, re) (span 1 only): the reference's
+// Cnt.RNG_STRT / RNG_END mode, in which projections cover the ring pairs inside the range,
+// sinograms are numbered by the range's own span-1 Michelogram and images hold the axial
+// voxel slab [vz0, vz0 + nvz) with nvz = 2 (re - rs) - 1 (prj/src/prjf.cu:209-320,
+// prjb.cu:190-308, mmraux.py:566-617).  Every ray is one of the geometry's own rays, so
+// the walk checks of nb_geom_create cover it.
+struct nb_rings {
+  int device;
+  int rs, re;
+  int nrays;         // rays of the range = its span-1 sinograms
+  int vz0, nvz;
+  nb_ray *d_rays;    // [nrays], out1 = the range's sinogram of the ray
+  int16_t *d_bin1;   // [nrays] ray of each of the range's sinograms
 };
 
 // ---- host-side error plumbing (nb_capi.cu) ----

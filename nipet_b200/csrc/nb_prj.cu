@@ -37,6 +37,33 @@ __global__ void k_from_col128(float *__restrict__ dst, const float *__restrict__
   for (int z = lane; z < NB_IMZ; z += 32) d[z] = s[nb_zi(z)];
 }
 
+// Images of a reduced ring range hold the axial slab [vz0, vz0 + nvz) only
+// ([320][320][nvz], z fastest).  Expand: the slab into a full col128 image, zero elsewhere
+// (prjf.cu:19-29 imExpand); reduce: the slab out of a col128 image (prjb.cu:19-29
+// imReduce).  One warp per column.
+__global__ void k_slab_to_col128(float *__restrict__ dst, const float *__restrict__ src,
+                                 int nvz, int vz0) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= NB_NCOL) return;
+  const float *s = src + (size_t)wid * nvz;
+  float *d = dst + (size_t)wid * NB_COLW;
+  for (int z = lane; z < NB_COLW; z += 32) {
+    const int zr = z - vz0;
+    d[nb_zi(z)] = (z < NB_IMZ && zr >= 0 && zr < nvz) ? s[zr] : 0.f;
+  }
+}
+
+__global__ void k_col128_to_slab(float *__restrict__ dst, const float *__restrict__ src,
+                                 int nvz, int vz0) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= NB_NCOL) return;
+  const float *s = src + (size_t)wid * NB_COLW;
+  float *d = dst + (size_t)wid * nvz;
+  for (int z = lane; z < nvz; z += 32) d[z] = s[nb_zi(vz0 + z)];
+}
+
 __global__ void k_osem_rs(float *__restrict__ rs, const float *__restrict__ r,
                           const float *__restrict__ s, const float *__restrict__ an_a,
                           const float *__restrict__ an_n, size_t n) {
@@ -130,6 +157,8 @@ PrjArgs base_args(nb_geom *g, const int32_t *subs, int nprj, int span) {
   a.subs = subs;
   a.nprj = subs ? nprj : g->naw;
   a.naw = g->naw;
+  a.nrays = NB_NRAYS;
+  a.nout = span == 11 ? NB_NSN11 : NB_NSN1;
   a.span = span;
   a.fxbits = g->fxbits;
   a.err = g->d_err;
@@ -222,6 +251,66 @@ extern "C" int nb_bprj(nb_geom *g, float *im, const float *sino, const int32_t *
   st = nb_bprj_col128(g, g->d_scratch128, sino, subs, nprj, span, stream);
   if (st) return st;
   return nb_col128_to_im(im, g->d_scratch128, 1, stream);
+}
+
+// Span-1 projections over a reduced ring range (gpu_fprj / gpu_bprj with Cnt.RNG_STRT /
+// RNG_END, prjf.cu:209-320, prjb.cu:190-308): images are the range's axial slab
+// [320][320][nvz], sinograms [nprj][nsino] numbered by the range's Michelogram.  The slab
+// is expanded into the handle's col128 scratch with zeros elsewhere (as the reference's
+// imExpand) and the persistent projector walks only the range's rays.
+static int check_rings(nb_geom *g, const nb_rings *rr) {
+  NB_REQUIRE(rr != nullptr, "NULL ring-range handle");
+  NB_REQUIRE(rr->device == g->device, "ring-range handle and geometry on different devices");
+  NB_REQUIRE(rr->vz0 >= 0 && rr->nvz > 0 && rr->vz0 + rr->nvz <= NB_IMZ,
+             "ring-range handle with a bad axial slab");
+  return NB_OK;
+}
+
+extern "C" int nb_fprj_rings(nb_geom *g, const nb_rings *rr, float *sino, const float *im,
+                             const int32_t *subs, int nprj, int att, void *stream) {
+  int st = check_common(g, nprj, subs, 1);
+  if (st) return st;
+  st = check_rings(g, rr);
+  if (st) return st;
+  NB_REQUIRE(sino && im, "nb_fprj_rings: NULL sino or image");
+  NB_REQUIRE(att == 0 || att == 1, "att must be 0 or 1");
+  cudaStream_t s = (cudaStream_t)stream;
+  k_slab_to_col128<<<(NB_NCOL * 32 + 255) / 256, 256, 0, s>>>(g->d_scratch128, im, rr->nvz,
+                                                               rr->vz0);
+  NB_CUDA(cudaGetLastError());
+  PrjArgs a = base_args(g, subs, nprj, 1);
+  a.rays = rr->d_rays;
+  a.bin1 = rr->d_bin1;
+  a.nrays = rr->nrays;
+  a.nout = rr->nrays;
+  a.att = att;
+  a.img = g->d_scratch128;
+  a.sino = sino;
+  return launch_project<MODE_FWD, CH_FWD>(g, a, s);
+}
+
+extern "C" int nb_bprj_rings(nb_geom *g, const nb_rings *rr, float *im, const float *sino,
+                             const int32_t *subs, int nprj, void *stream) {
+  int st = check_common(g, nprj, subs, 1);
+  if (st) return st;
+  st = check_rings(g, rr);
+  if (st) return st;
+  NB_REQUIRE(sino && im, "nb_bprj_rings: NULL sino or image");
+  cudaStream_t s = (cudaStream_t)stream;
+  NB_CUDA(cudaMemsetAsync(g->d_scratch128, 0, sizeof(float) * NB_IMG_COL128, s));
+  PrjArgs a = base_args(g, subs, nprj, 1);
+  a.rays = rr->d_rays;
+  a.bin1 = rr->d_bin1;
+  a.nrays = rr->nrays;
+  a.nout = rr->nrays;
+  a.bimg = g->d_scratch128;
+  a.sino_in = sino;
+  st = launch_project<MODE_BWD, CH_BWD>(g, a, s);
+  if (st) return st;
+  k_col128_to_slab<<<(NB_NCOL * 32 + 255) / 256, 256, 0, s>>>(im, g->d_scratch128, rr->nvz,
+                                                               rr->vz0);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
 }
 
 extern "C" int nb_osem_rs(float *rs, const float *rsng, const float *ssng, const float *asng,

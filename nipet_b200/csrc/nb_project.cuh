@@ -6,8 +6,9 @@
 //
 // B200 design
 //  * Persistent grid, one 1024-thread CTA per SM.  A CTA owns one LOR (a transaxial
-//    sinogram bin) at a time and computes all 4084 rays (span-1 ring pairs) of it;
-//    thread t handles rays t, t+1024, t+2048, t+3072 of the canonical ray order.
+//    sinogram bin) at a time and computes all 4084 rays (span-1 ring pairs) of it, or
+//    the rays of a reduced ring range (PrjArgs::rays / nrays); thread t handles rays t,
+//    t+1024, t+2048, t+3072 of the ray table's order.
 //  * The LOR's voxel columns (512 B each in the col128 layout) are streamed into shared
 //    memory in chunks of CH columns with TMA bulk copies (cp.async.bulk + mbarrier),
 //    double buffered, so every voxel read of the walk is a shared-memory load.
@@ -48,6 +49,8 @@ struct PrjArgs {
   const int32_t *subs;
   int nprj;
   int naw;
+  int nrays;             // rays of `rays` (4084, or those of a reduced ring range)
+  int nout;              // sinograms per row (837, 4084, or a reduced range's count)
   int span;              // 1 or 11
   int att;               // forward: 0 emission, 1 attenuation
   const float *img;      // col128 image read by forward passes
@@ -159,7 +162,7 @@ __device__ __forceinline__ void rays_init(const PrjArgs &a, const float4 h, RayS
   for (int r = 0; r < RPT; r++) {
     const int ray = threadIdx.x + NT * r;
     S.acc[r] = 0.f;
-    if (ray < NB_NRAYS) {
+    if (ray < a.nrays) {
       nb_axial A;
       nb_axial_setup(a.rays[ray], h.y, h.x, h.z, A);
       S.zo[r] = 4 * nb_zi(A.w);
@@ -324,7 +327,7 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
 
   const int tid = threadIdx.x;
   const bool warp0 = tid < 32;
-  const int nout = a.span == 11 ? NB_NSN11 : NB_NSN1;
+  const int nout = a.nout;
 
   if (tid == 0) {
     nb_mbar_init(&bars[0], 1);
@@ -378,7 +381,7 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
         for (int r = 0; r < RPT; r++) {
           const int ray = tid + NT * r;
           float v = 0.f;
-          if (ray < NB_NRAYS) {
+          if (ray < a.nrays) {
             const nb_ray R = a.rays[ray];
             const int o = a.span == 11 ? R.out11 : R.out1;
             const size_t row = a.in_by_lor ? (size_t)J.lor : (size_t)J.p;
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(NT, 1) k_project(const PrjArgs a) {
 #pragma unroll
       for (int r = 0; r < RPT; r++) {
         const int ray = tid + NT * r;
-        if (ray < NB_NRAYS) {
+        if (ray < a.nrays) {
           float v = S.acc[r] * ray_s(a, ray, h.y);
           if (MODE == MODE_FWD && a.att == 1) {
             v = expf(-v);

@@ -13,7 +13,7 @@ import torch
 from . import _lib
 
 __all__ = ['Geometry', 'get_geometry', 'to_device', 'dev_ptr', 'stream_ptr', 'device_of',
-           'projector']
+           'projector', 'RingSet', 'get_rings', 'full_axial_lut', 'is_reduced']
 
 
 def device_of(Cnt: dict | None = None, device=None) -> torch.device:
@@ -146,6 +146,89 @@ def get_geometry(txLUT: dict, axLUT: dict, device: torch.device) -> Geometry:
             g._lut_refs = (txLUT['crs'], txLUT['s2c'], axLUT['li2rng'], axLUT['li2sn'],
                            axLUT['li2sn1'], axLUT['li2nos'])
         return g
+
+
+_FULL_AX: dict = {}
+
+
+def full_axial_lut(Cnt: dict) -> dict:
+    """The axial LUTs of all 64 rings for the scanner constants in `Cnt` (the geometry a
+    reduced ring range is cut from), built once per set of constants."""
+    from .geometry import axial_lut
+    key = (Cnt['NRNG'], Cnt['MRD'], Cnt['AXR'], tuple(Cnt['SEG']), tuple(Cnt['MNRD']),
+           tuple(Cnt['MXRD']), Cnt['NSN11'], Cnt['NSEG0'])
+    with _LOCK:
+        ax = _FULL_AX.get(key)
+    if ax is None:
+        ax = axial_lut(dict(Cnt, SPN=11, RNG_STRT=0, RNG_END=Cnt['NRNG']))
+        with _LOCK:
+            ax = _FULL_AX.setdefault(key, ax)
+    return ax
+
+
+def is_reduced(Cnt: dict) -> bool:
+    """True when `Cnt` selects a reduced axial ring range (span-1 RNG_STRT / RNG_END)."""
+    return (int(Cnt.get('RNG_STRT', 0)) != 0
+            or int(Cnt.get('RNG_END', Cnt.get('NRNG', 64))) != int(Cnt.get('NRNG', 64)))
+
+
+class RingSet:
+    """The rays of a reduced ring range [rs, re) (nb_rings handle) on a geometry: built
+    from the range's own axial LUTs (those `mmraux.reduce_rings` puts in `axLUT`)."""
+
+    def __init__(self, geom: Geometry, rs: int, re: int, axLUT: dict):
+        lib = _lib.load()
+        li2rng = np.ascontiguousarray(axLUT['li2rng'], dtype=np.float32)
+        li2sn1 = np.ascontiguousarray(axLUT['li2sn1'], dtype=np.int16)
+        if li2rng.ndim != 2 or li2rng.shape[1] != 2 or li2sn1.shape != li2rng.shape:
+            raise ValueError('li2rng / li2sn1 must be [nli2r, 2] arrays')
+        h = C.c_void_p()
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        with torch.cuda.device(geom.device):
+            _lib.check(lib.nb_rings_create(geom.handle, int(rs), int(re), p(li2rng), p(li2sn1),
+                                           li2rng.shape[0], C.byref(h)))
+        self.handle = h
+        self.geom = geom
+        n, z0, nz = C.c_int(), C.c_int(), C.c_int()
+        _lib.check(lib.nb_rings_info(h, C.byref(n), C.byref(z0), C.byref(nz)))
+        self.rs, self.re = int(rs), int(re)
+        self.nsino, self.vz0, self.nvz = n.value, z0.value, nz.value
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            self._lib.nb_rings_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_RINGS: dict = {}
+
+
+def get_rings(txLUT: dict, axLUT: dict, Cnt: dict, device) -> RingSet:
+    """The full geometry and the ray set of the reduced ring range in `Cnt`
+    (`RNG_STRT`/`RNG_END`, span 1), for the range's axial LUTs `axLUT`; cached per device,
+    range and LUT content."""
+    if int(Cnt['SPN']) != 1:
+        raise ValueError('the reduced axial FOV only works in span-1')
+    rs, re = int(Cnt['RNG_STRT']), int(Cnt['RNG_END'])
+    dev = torch.device(device)
+    geom = get_geometry(txLUT, full_axial_lut(Cnt), dev)
+    li2rng = np.ascontiguousarray(axLUT['li2rng'], dtype=np.float32)
+    li2sn1 = np.ascontiguousarray(axLUT['li2sn1'], dtype=np.int16)
+    key = (str(dev), id(geom), rs, re, li2rng.tobytes(), li2sn1.tobytes())
+    with _LOCK:
+        r = _RINGS.get(key)
+    if r is None:
+        r = RingSet(geom, rs, re, axLUT)
+        with _LOCK:
+            r = _RINGS.setdefault(key, r)
+    return r
 
 
 def projector(params: dict, device):

@@ -13,7 +13,39 @@ from .geometry import (axial_lut, get_mmr_constants, get_mmrparams, mmrinit, nsi
                        span1_span11, transaxial_lut)
 
 __all__ = ['remgaps', 'putgaps', 'axial_lut', 'transaxial_lut', 'mmrinit', 'get_mmrparams',
-           'get_mmr_constants', 'span1_span11']
+           'get_mmr_constants', 'span1_span11', 'reduce_rings']
+
+
+def reduce_rings(pars: dict, rs: int = 0, re: int = 64) -> None:
+    """Switch `pars` (a scanner_params dict, changed in place) to the reduced axial FOV of
+    rings [rs, re) (`mmraux.py:566-617`): span 1; `Cnt['RNG_STRT']`, `Cnt['RNG_END']` = rs,
+    re; the range's axial voxel count `rSO_IMZ` = `rSZ_IMZ` = 2(re-rs)-1; `rNRNG` = re-rs;
+    `rNSN1` = (re-rs)^2 (the count before the 64-ring correction, as the reference stores
+    it); and `axLUT` replaced by the range's axial LUTs with `rLUT`, the full span-1 sinogram
+    of each of the range's sinograms (looked up in the `axLUT` the call replaces).  The
+    number of rings must be even and positive."""
+    if not (0 <= rs < re <= pars['Cnt']['NRNG']) or (re - rs) % 2:
+        raise ValueError('The resulting number of rings has to be even and start ring (rs)'
+                         ' smaller than end ring (re)')
+    Cnt = pars['Cnt']
+    Cnt['SPN'] = 1
+    Cnt['RNG_STRT'] = rs
+    Cnt['RNG_END'] = re
+    nvz = 2 * (re - 1) - 2 * rs + 1
+    Cnt['rSO_IMZ'] = nvz
+    Cnt['rSZ_IMZ'] = nvz
+    n = re - rs
+    Cnt['rNRNG'] = n
+    Cnt['rNSN1'] = n * n
+    nsn = n * n - (12 if n == 64 else 0)
+    rax = axial_lut(Cnt)
+    msn1_r = rax['Msn1']
+    msn1 = np.asarray(pars['axLUT']['Msn1'])
+    sel = msn1_r >= 0
+    rlut = np.zeros(nsn, dtype=np.int16)
+    rlut[msn1_r[sel]] = msn1[sel]
+    rax['rLUT'] = rlut
+    pars['axLUT'] = rax
 
 
 def _aw2ali(txLUT, dev):

@@ -41,9 +41,12 @@ def frwd_prj(im, scanner_params, isub=ISUB_DEFAULT, dev_out=False, attenuation=F
     nsinos = nsinos_for(Cnt)
     is_np = _np_in(im)
     shp = tuple(im.shape)
-    if shp == (Cnt['SO_IMZ'], Cnt['SO_IMY'], Cnt['SO_IMX']):
-        ims = convert2dev(np.asarray(im if is_np else im.cpu().numpy()), Cnt)
-    elif shp == (Cnt['SZ_IMX'], Cnt['SZ_IMY'], Cnt['SZ_IMZ']):
+    # the full axial extent, or the slab of a reduced ring range (`reduce_rings`)
+    nzs = {Cnt['SO_IMZ'], Cnt.get('rSO_IMZ', Cnt['SO_IMZ'])}
+    nzd = {Cnt['SZ_IMZ'], Cnt.get('rSZ_IMZ', Cnt['SZ_IMZ'])}
+    if shp[1:] == (Cnt['SO_IMY'], Cnt['SO_IMX']) and shp[0] in nzs:
+        ims = convert2dev(np.asarray(im) if is_np else im, Cnt)   # a tensor stays on its device
+    elif shp[:2] == (Cnt['SZ_IMX'], Cnt['SZ_IMY']) and shp[2] in nzd:
         ims = im
     else:
         raise ValueError('wrong image size; it has to be one of these: (z,y,x) = (127,344,344)'
@@ -92,7 +95,7 @@ def back_prj(sino, scanner_params, isub=ISUB_DEFAULT, dev_out=False, output=None
     else:
         raise ValueError('Unexpected shape of the input sinogram.')
     dev = device_of(Cnt)
-    out_shape = (Cnt['SZ_IMX'], Cnt['SZ_IMY'], Cnt['SZ_IMZ'])
+    out_shape = petprj.image_shape_of(Cnt)   # the range's axial slab with reduced rings
     bimg = torch.zeros(out_shape, device=dev) if output is None else output
     petprj.bprj(bimg, sinog, txLUT, axLUT, isub, Cnt, sync=sync)
     if not dev_out:

@@ -14,14 +14,15 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import STAGED_COPY_BYTES, dev_ptr, device_of, get_geometry, stream_ptr, to_device
+from .device import (STAGED_COPY_BYTES, dev_ptr, device_of, get_geometry, get_rings,
+                     is_reduced, stream_ptr, to_device)
 
 _TORCH2NP = {torch.float32: np.dtype('float32'), torch.float64: np.dtype('float64'),
              torch.int32: np.dtype('int32'), torch.int16: np.dtype('int16'),
              torch.uint16: np.dtype('uint16'), torch.uint8: np.dtype('uint8'),
              torch.uint32: np.dtype('uint32')}
 
-__all__ = ['tprj', 'fprj', 'bprj', 'osem', 'nsinos_of', 'NLI2R', 'NAW']
+__all__ = ['tprj', 'fprj', 'bprj', 'osem', 'nsinos_of', 'image_shape_of', 'NLI2R', 'NAW']
 
 NAW = 68516
 NLI2R = 2074
@@ -30,15 +31,28 @@ COL128 = 320 * 320 * 128
 
 
 def nsinos_of(Cnt: dict) -> int:
+    """Sinograms per row of the projectors for `Cnt`: 837 at span 11, 4084 at span 1, and
+    (re - rs)^2 for a reduced ring range [RNG_STRT, RNG_END) (span 1 only)."""
     span = Cnt['SPN']
     if span == 11:
+        if is_reduced(Cnt):
+            raise ValueError('the reduced axial FOV only works in span-1')
         return 837
     if span == 1:
-        if Cnt.get('RNG_STRT', 0) != 0 or Cnt.get('RNG_END', 64) != 64:
-            raise NotImplementedError('reduced axial ring ranges (span-1 RNG_STRT/RNG_END) are '
-                                      'not provided by nipet_b200')
-        return 4084
+        rs, re = int(Cnt.get('RNG_STRT', 0)), int(Cnt.get('RNG_END', 64))
+        if not 0 <= rs < re <= 64:
+            raise ValueError(f'bad ring range [{rs}, {re})')
+        n = re - rs
+        return n * n - (12 if n == 64 else 0)
     raise ValueError(f'unsupported span {span} (the projectors support 1 and 11)')
+
+
+def image_shape_of(Cnt: dict) -> tuple:
+    """Image shape of the projectors for `Cnt`: (320, 320, 127), or (320, 320, 2(re-rs)-1)
+    for a reduced ring range (the axial slab the range sees)."""
+    if int(Cnt['SPN']) == 1 and is_reduced(Cnt):
+        return (320, 320, 2 * (int(Cnt['RNG_END']) - int(Cnt['RNG_STRT'])) - 1)
+    return IMG_SHAPE
 
 
 def _subs_arg(subs, device):
@@ -90,21 +104,33 @@ def tprj(sino, im, tv, tt, txLUT, cnst):
 def fprj(sino, im, txLUT, axLUT, subs, cnst, att, sync=True):
     """Forward projection into `sino` (`[Nprj|68516, nsinos]` float32, overwritten), as
     `petprj.fprj` (`prj_module.cu:232-425`, `prjf.cu:209-320`).  `att=1` gives
-    attenuation factors exp(-line integral)."""
+    attenuation factors exp(-line integral).
+
+    With a reduced ring range in `cnst` (span 1, `RNG_STRT`/`RNG_END` as
+    `mmraux.reduce_rings` sets them, and that function's `axLUT`) the image is the range's
+    axial slab `[320, 320, 2(re-rs)-1]` and the sinograms are the range's `(re-rs)^2`
+    (`prjf.cu:209-320` with `imExpand`)."""
     dev = device_of(cnst)
     nsn = nsinos_of(cnst)
-    g = get_geometry(txLUT, axLUT, dev)
+    ishape = image_shape_of(cnst)
+    rings = get_rings(txLUT, axLUT, cnst, dev) if ishape != IMG_SHAPE else None
+    g = rings.geom if rings is not None else get_geometry(txLUT, axLUT, dev)
     d_subs, nprj = _subs_arg(subs, dev)
     if tuple(np.shape(sino)) != (nprj, nsn):
         raise ValueError(f'sino must have shape {(nprj, nsn)}, got {tuple(np.shape(sino))}')
-    if tuple(np.shape(im)) != IMG_SHAPE:
-        raise ValueError(f'image must have shape {IMG_SHAPE}')
+    if tuple(np.shape(im)) != ishape:
+        raise ValueError(f'image must have shape {ishape}')
     d_im = to_device(im, np.float32, dev)
     out = sino if (isinstance(sino, torch.Tensor) and sino.is_cuda and sino.is_contiguous()
                    and sino.dtype == torch.float32) else torch.empty((nprj, nsn), device=dev)
-    _lib.check(_lib.load().nb_fprj(g.handle, dev_ptr(out), dev_ptr(d_im),
-                                   dev_ptr(d_subs) if d_subs is not None else None, nprj,
-                                   int(cnst['SPN']), int(att), stream_ptr(dev)))
+    sp = dev_ptr(d_subs) if d_subs is not None else None
+    if rings is not None:
+        _lib.check(_lib.load().nb_fprj_rings(g.handle, rings.handle, dev_ptr(out),
+                                             dev_ptr(d_im), sp, nprj, int(att),
+                                             stream_ptr(dev)))
+    else:
+        _lib.check(_lib.load().nb_fprj(g.handle, dev_ptr(out), dev_ptr(d_im), sp, nprj,
+                                       int(cnst['SPN']), int(att), stream_ptr(dev)))
     if sync:
         g.check()
     _writeback(sino, out)
@@ -112,21 +138,28 @@ def fprj(sino, im, txLUT, axLUT, subs, cnst, att, sync=True):
 
 def bprj(bimg, sino, txLUT, axLUT, subs, cnst, sync=True):
     """Back projection into `bimg` (`[320,320,127]` float32, overwritten), as `petprj.bprj`
-    (`prj_module.cu:430-608`, `prjb.cu:190-308`)."""
+    (`prj_module.cu:430-608`, `prjb.cu:190-308`).  A reduced ring range gives the range's
+    axial slab `[320, 320, 2(re-rs)-1]` (`imReduce`), as in `fprj`."""
     dev = device_of(cnst)
     nsn = nsinos_of(cnst)
-    g = get_geometry(txLUT, axLUT, dev)
+    ishape = image_shape_of(cnst)
+    rings = get_rings(txLUT, axLUT, cnst, dev) if ishape != IMG_SHAPE else None
+    g = rings.geom if rings is not None else get_geometry(txLUT, axLUT, dev)
     d_subs, nprj = _subs_arg(subs, dev)
     if tuple(np.shape(sino)) != (nprj, nsn):
         raise ValueError(f'sino must have shape {(nprj, nsn)}, got {tuple(np.shape(sino))}')
-    if tuple(np.shape(bimg)) != IMG_SHAPE:
-        raise ValueError(f'image must have shape {IMG_SHAPE}')
+    if tuple(np.shape(bimg)) != ishape:
+        raise ValueError(f'image must have shape {ishape}')
     d_sino = to_device(sino, np.float32, dev)
     out = bimg if (isinstance(bimg, torch.Tensor) and bimg.is_cuda and bimg.is_contiguous()
-                   and bimg.dtype == torch.float32) else torch.empty(IMG_SHAPE, device=dev)
-    _lib.check(_lib.load().nb_bprj(g.handle, dev_ptr(out), dev_ptr(d_sino),
-                                   dev_ptr(d_subs) if d_subs is not None else None, nprj,
-                                   int(cnst['SPN']), stream_ptr(dev)))
+                   and bimg.dtype == torch.float32) else torch.empty(ishape, device=dev)
+    sp = dev_ptr(d_subs) if d_subs is not None else None
+    if rings is not None:
+        _lib.check(_lib.load().nb_bprj_rings(g.handle, rings.handle, dev_ptr(out),
+                                             dev_ptr(d_sino), sp, nprj, stream_ptr(dev)))
+    else:
+        _lib.check(_lib.load().nb_bprj(g.handle, dev_ptr(out), dev_ptr(d_sino), sp, nprj,
+                                       int(cnst['SPN']), stream_ptr(dev)))
     if sync:
         g.check()
     _writeback(bimg, out)
@@ -161,6 +194,9 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     span = int(cnst['SPN'])
     if span not in (1, 11):
         raise ValueError(f'unrecognised span {span}')
+    if is_reduced(cnst):
+        # recon.cu:318-521 sizes every sinogram and image for all 64 rings
+        raise ValueError('osem runs over all 64 rings; switch off the reduced rings mode')
     k = np.ascontiguousarray(np.asarray(krnl.cpu() if isinstance(krnl, torch.Tensor) else krnl,
                                         dtype=np.float32).reshape(-1))
     use_psf = k.size > 0 and k[0] >= 0

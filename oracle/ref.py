@@ -44,9 +44,11 @@ def load():
         lib.ref_remgaps.argtypes = [P, P, I, P]
         lib.ref_sct.argtypes = [P, P, P, P, P, P, C.c_float, C.c_float] + [P] * 9 + [I]
         lib.ref_putgaps.argtypes = [P, P, P, I, I]
+        lib.ref_fprj_rng.argtypes = [P, P, P, I, I, I, I, P, P, P, P, P, P, I, P]
+        lib.ref_bprj_rng.argtypes = [P, P, P, I, I, I, P, P, P, P, P, I, P]
         for f in (lib.ref_fprj, lib.ref_bprj, lib.ref_osem, lib.ref_tables, lib.ref_lminfo,
                   lib.ref_hist, lib.ref_psf, lib.ref_randoms, lib.ref_remgaps,
-                  lib.ref_putgaps, lib.ref_sct):
+                  lib.ref_putgaps, lib.ref_sct, lib.ref_fprj_rng, lib.ref_bprj_rng):
             f.restype = I
         _lib = lib
     return _lib
@@ -99,6 +101,47 @@ def bprj(params, sino, subs=None, span=11):
     ms = C.c_float()
     _check(load().ref_bprj(_p(out), _p(sino), _p(s), nprj, span, _p(L.li2rng), _p(L.li2sn),
                            _p(L.li2nos), _p(L.s2c), _p(L.crs), L.ncrs, C.byref(ms)), 'bprj')
+    return out, ms.value
+
+
+def _range_of(params):
+    Cnt = params['Cnt']
+    rs, re = int(Cnt['RNG_STRT']), int(Cnt['RNG_END'])
+    n = re - rs
+    return rs, re, n * n - (12 if n == 64 else 0), (320, 320, 2 * n - 1)
+
+
+def fprj_rng(params, im, subs=None, att=0):
+    """Reference gpu_fprj in the reduced-rings mode of `params` (after
+    `mmraux.reduce_rings`): im [320][320][nvz] -> (sino [nprj][nsino], device ms)."""
+    rs, re, nsn, shp = _range_of(params)
+    L = _Luts(params, 1)
+    im = np.ascontiguousarray(im, np.float32).reshape(shp)
+    s = None if subs is None else np.ascontiguousarray(subs, np.int32).reshape(-1)
+    nprj = NAW if s is None else s.size
+    out = np.empty((nprj, nsn), np.float32)
+    ms = C.c_float()
+    _check(load().ref_fprj_rng(_p(out), _p(im), _p(s), nprj, rs, re, att, _p(L.li2rng),
+                               _p(L.li2sn), _p(L.li2nos), _p(L.s2c), _p(L.aw2ali), _p(L.crs),
+                               L.ncrs, C.byref(ms)), 'fprj (reduced rings)')
+    return out, ms.value
+
+
+def bprj_rng(params, sino, subs=None):
+    """Reference gpu_bprj in the reduced-rings mode of `params`: sino [nprj][nsino] ->
+    (image [320][320][nvz], device ms)."""
+    rs, re, nsn, shp = _range_of(params)
+    L = _Luts(params, 1)
+    sino = np.ascontiguousarray(sino, np.float32)
+    s = None if subs is None else np.ascontiguousarray(subs, np.int32).reshape(-1)
+    nprj = NAW if s is None else s.size
+    if sino.shape != (nprj, nsn):
+        raise ValueError('sinogram shape does not match the subset and ring range')
+    out = np.empty(shp, np.float32)
+    ms = C.c_float()
+    _check(load().ref_bprj_rng(_p(out), _p(sino), _p(s), nprj, rs, re, _p(L.li2rng),
+                               _p(L.li2sn), _p(L.li2nos), _p(L.s2c), _p(L.crs), L.ncrs,
+                               C.byref(ms)), 'bprj (reduced rings)')
     return out, ms.value
 
 

@@ -161,6 +161,86 @@ int ref_bprj(float *im, const float *sino, const int *subs, int nprj, int span,
   return (int)tx.err;
 }
 
+// The reduced-rings mode of the same routines (span 1, Cnt.RNG_STRT = rs, Cnt.RNG_END = re,
+// with the range's axial LUTs from mmraux.reduce_rings): the image is the range's axial
+// slab [320][320][nvz], nvz = 2 (re - rs) - 1, the sinogram [nprj][nsino] with
+// nsino = (re - rs)^2 (less 12 for 64 rings).  gpu_fprj / gpu_bprj expand and reduce the
+// slab themselves (prjf.cu:19-29, :255-266; prjb.cu:19-29, :286-296).
+int ref_fprj_rng(float *sino, const float *im, const int *subs, int nprj, int rs, int re,
+                 int att, const float *li2rng, const int16_t *li2sn1, const int8_t *li2nos,
+                 const int16_t *s2c, const int *aw2ali, const float *crs, int ncrs, float *ms) {
+  const int n = re - rs;
+  const int nsn = n * n - (n == NRINGS ? 12 : 0);
+  const size_t nvox = (size_t)SZ_IMX * SZ_IMY * (2 * n - 1);
+  Cnst c = make_cnst(1);
+  c.RNG_STRT = (char)rs;
+  c.RNG_END = (char)re;
+  Tx tx(crs, ncrs, s2c, subs, nprj);
+  float *d_im = nullptr, *d_sn = nullptr;
+  tx.chk(cudaMalloc(&d_im, nvox * sizeof(float)));
+  tx.chk(cudaMemcpy(d_im, im, nvox * sizeof(float), cudaMemcpyHostToDevice));
+  tx.chk(cudaMalloc(&d_sn, (size_t)nprj * nsn * sizeof(float)));
+  if (tx.err != cudaSuccess) return (int)tx.err;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  gpu_fprj(d_sn, d_im, const_cast<float *>(li2rng), const_cast<short *>(li2sn1),
+           reinterpret_cast<char *>(const_cast<int8_t *>(li2nos)), tx.s2c,
+           const_cast<int *>(aw2ali), tx.crs, tx.subs, tx.tt, tx.tv, nprj, AW, c, (char)att,
+           false);
+  cudaEventRecord(e1, 0);
+  tx.chk(cudaEventSynchronize(e1));
+  tx.chk(cudaGetLastError());
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  tx.chk(cudaMemcpy(sino, d_sn, (size_t)nprj * nsn * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_im);
+  cudaFree(d_sn);
+  return (int)tx.err;
+}
+
+int ref_bprj_rng(float *im, const float *sino, const int *subs, int nprj, int rs, int re,
+                 const float *li2rng, const int16_t *li2sn1, const int8_t *li2nos,
+                 const int16_t *s2c, const float *crs, int ncrs, float *ms) {
+  const int n = re - rs;
+  const int nsn = n * n - (n == NRINGS ? 12 : 0);
+  const size_t nvox = (size_t)SZ_IMX * SZ_IMY * (2 * n - 1);
+  Cnst c = make_cnst(1);
+  c.RNG_STRT = (char)rs;
+  c.RNG_END = (char)re;
+  Tx tx(crs, ncrs, s2c, subs, nprj);
+  float *d_im = nullptr, *d_sn = nullptr;
+  // gpu_bprj back-projects into a full-size image of its own and copies the slab into d_im
+  tx.chk(cudaMalloc(&d_im, (n == NRINGS ? (size_t)SZ_IMX * SZ_IMY * SZ_IMZ : nvox) *
+                               sizeof(float)));
+  tx.chk(cudaMalloc(&d_sn, (size_t)nprj * nsn * sizeof(float)));
+  tx.chk(cudaMemcpy(d_sn, sino, (size_t)nprj * nsn * sizeof(float), cudaMemcpyHostToDevice));
+  if (tx.err != cudaSuccess) return (int)tx.err;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, 0);
+  gpu_bprj(d_im, d_sn, const_cast<float *>(li2rng), const_cast<short *>(li2sn1),
+           reinterpret_cast<char *>(const_cast<int8_t *>(li2nos)), tx.s2c, tx.crs, tx.subs,
+           tx.tt, tx.tv, nprj, c, false);
+  cudaEventRecord(e1, 0);
+  tx.chk(cudaEventSynchronize(e1));
+  tx.chk(cudaGetLastError());
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  if (ms) *ms = t;
+  tx.chk(cudaMemcpy(im, d_im, nvox * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_im);
+  cudaFree(d_sn);
+  return (int)tx.err;
+}
+
 // One OSEM iteration over all subsets by the reference's osem(), updating `img`
 // ([320][320][127], host) in place, as petprj.osem does; psf: the [3][17] resolution
 // kernel, or NULL for none.  subs is the

@@ -57,6 +57,30 @@ def test_scatter_model_matches_reference(params, cuda_device, sct_inputs, span):
         assert not s3d[4084:].any()
 
 
+@pytest.mark.skipif(not ref.available(), reason='reference CUDA build (oracle/_ref) not present')
+def test_scatter_model_time_against_reference(params, cuda_device, sct_inputs, capsys):
+    """Device time of one scatter-model call (span 11, second call, CUDA events around
+    `scatter_presino`: ray sums, scatter probabilities, pre-sinograms) against the
+    reference's prob_scatt on the same inputs (the harness's events around the call); the
+    times are printed (pytest -s)."""
+    Cnt = dict(params['Cnt'], SPN=11)
+    sp = dict(params, Cnt=Cnt)
+    lut = mmrsct.get_sctLUT(sp)
+    mu, msk, em = sct_inputs
+    ours = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mmrsct.scatter_presino(mu, msk, em, lut, sp, device=cuda_device, return_raw=True)
+        e1.record()
+        e1.synchronize()
+        ours.append(e0.elapsed_time(e1))
+    theirs = [ref.sct(sp, mu, msk, em, lut, span=11)[2] for _ in range(2)]
+    with capsys.disabled():
+        print(f'\nscatter model ms: this package {ours}, reference prob_scatt {theirs}')
+    assert ours[1] < min(theirs)
+
+
 def test_vsm_scaled_estimate(params, cuda_device, sct_inputs):
     """The whole estimate on a synthetic span-11 scan: prompts = trues + randoms + a known
     multiple of the model's own scatter; the scaled estimate must recover that multiple in
