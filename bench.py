@@ -571,18 +571,51 @@ def run_diff(args, ws, rank, dev):
             et.append(time.perf_counter() - t)
     te = _max_over_ranks(float(np.mean(et)), ws, dev)
     # roofline: one step = 2 attenuation projections (weights, recomputed in the backward
-    # pass) + 8 forward + 8 back projections: 4 B per voxel read / update each
+    # pass) + the batched forward and back projections of the 8 images.  Bound: the
+    # shared-memory pipe, with the step's wavefronts from one-kernel ncu counts of the same
+    # launches (profiles/traffic.json, `profile_cases.py diffdyn`) over the step's time (the
+    # step also holds the layout conversions and the NLL); the survey's algorithmic 4 B per
+    # voxel read / update and the real DRAM bytes ride along
     V = prj.geom.count_reads()
-    achieved = (2 + 2 * nimg) * 4 * V / t_step / 1e9
+    alg = (2 + 2 * nimg) * 4 * V / t_step / 1e9
     peak, peak_kind = _peaks()
+    wfs = [_traffic(k) for k in ('diff_fwd8_smem_wavefronts', 'diff_bwd8_smem_wavefronts',
+                                 'att_fprj_smem_wavefronts')]
+    drs = [_traffic(k) for k in ('diff_fwd8', 'diff_bwd8', 'att_fprj')]
+    algorithmic = {'unit': 'GB/s', 'achieved': alg, 'frac_of_hbm_peak': alg / peak,
+                   'note': '4 B per Siddon voxel read and update, per image, as if every one '
+                           'came from HBM; above 1 because staged columns are reused from '
+                           'shared memory'}
+    if all(wfs):
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+        wstep = (wfs[0] + wfs[1]) * nimg / 8.0 + 2 * wfs[2]
+        dstep = ((drs[0] + drs[1]) * nimg / 8.0 + 2 * drs[2]) if all(drs) else None
+        roof = {'bound': 'smem', 'achieved': wstep / t_step, 'peak': nsm * mhz * 1e6,
+                'unit': 'wavefronts/s', 'frac': wstep / t_step / (nsm * mhz * 1e6),
+                'peak_kind': f'1 shared-memory wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz '
+                             '(median sampled clock)',
+                'traffic': dstep,
+                'kernel': 'k_osem_batch forward + backward modes (nb_fprj_batch / '
+                          'nb_bprj_batch, 4 images per walk) + 2 attenuation projections '
+                          '(k_project), whole step',
+                'wavefronts_per_step': wstep,
+                'hbm': ({'unit': 'GB/s', 'peak': peak, 'peak_kind': peak_kind,
+                         'achieved': dstep / t_step / 1e9,
+                         'frac': dstep / t_step / 1e9 / peak} if dstep else None),
+                'algorithmic': algorithmic}
+    else:
+        roof = {'bound': 'hbm', 'achieved': alg, 'peak': peak, 'unit': 'GB/s',
+                'frac': alg / peak, 'traffic': None, 'peak_kind': peak_kind,
+                'kernel': 'k_osem_batch forward + backward modes + attenuation k_project, '
+                          'whole step', 'note': 'algorithmic bytes: no capture in '
+                                                'profiles/traffic.json'}
     res = {'ms_per_step': t_step * 1e3, 'value': ws * nimg / t_step,
            'e2e': {'value': ws * nimg / te, 'unit': 'images/s',
                    'h2d_bytes_per_step': int(xh.numel() * 4),
                    'd2h_bytes_per_step': int(gh.numel() * 4 + 8)},
            'clocks': clocks, 'gpu_launches': launches,
-           'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                        'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
-                        'kernel': 'k_project forward + back (nb_fprj / nb_bprj), whole step'},
+           'roofline': roof,
            'config': {'workload': f'differentiable projector: {nimg} images 320x320x127, '
                                   'span-11 forward with attenuation x normalisation, Poisson '
                                   'NLL, gradient by the back projector', 'global_batch':
@@ -658,28 +691,43 @@ def run_dynamic(args, ws, rank, dev):
     t_it = float(np.mean(it_ms)) / 1e3
     achieved = bytes_iter / t_it / 1e9
     peak, peak_kind = _peaks()
-    wf8 = _traffic('osem_batch_8img_smem_wavefronts')
-    onchip = None
-    if wf8:
+    launch_s = t_it / len(br.subs)
+    algorithmic = {'unit': 'GB/s', 'achieved': achieved, 'frac_of_hbm_peak': achieved / peak,
+                   'bytes_per_launch_avg': bytes_iter / len(br.subs),
+                   'note': '4 B per Siddon voxel read and update per frame, as if every one '
+                           'came from HBM, + sinogram rows; above 1 because staged columns '
+                           'are reused from shared memory'}
+    # bound: the shared-memory pipe; wavefronts of one span-1 launch for one group of 4
+    # frames (ncu count of the same kernel shape on subset 0, `profile_cases.py diffdyn`),
+    # scaled by the launch's groups (every group walks every LOR of the subset; the 14
+    # subsets have the same number of LORs)
+    wf4 = _traffic('dyn_span1_4frames_smem_wavefronts')
+    dr4 = _traffic('dyn_span1_4frames')
+    if wf4 and br.bs == 4 and br.tile == 0:   # the captured shape
         nsm = torch.cuda.get_device_properties(dev).multi_processor_count
         mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
-        ach = wf8 * nfr / 8.0 / (t_it / len(br.subs))
-        onchip = {'bound': 'shared-memory pipe', 'unit': 'wavefronts/s', 'achieved': ach,
-                  'peak': nsm * mhz * 1e6, 'frac': ach / (nsm * mhz * 1e6),
-                  'wavefronts_per_launch': wf8 * nfr / 8.0,
-                  'peak_basis': f'1 wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz',
-                  'note': 'wavefronts of the 8-image span-11 capture scaled by frames (the '
-                          'same ray walks; span-1 sinogram rows are 4.9x longer)'}
-    roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-            'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
-            'kernel': f'k_osem_batch span 1 (nb_osem_batch_subset, {br.bs} frames per walk, '
-                      f'tile {br.tile})',
-            'bytes_per_launch_avg': bytes_iter / len(br.subs),
-            'launch_ms_avg': t_it * 1e3 / len(br.subs),
-            'note': 'achieved counts 4 B per Siddon voxel read/update as if from HBM; the '
-                    'kernel serves them from shared memory (see onchip); traffic: no span-1 '
-                    'capture',
-            'onchip': onchip}
+        wl = wf4 * ngroups
+        roof = {'bound': 'smem', 'achieved': wl / launch_s, 'peak': nsm * mhz * 1e6,
+                'unit': 'wavefronts/s', 'frac': wl / launch_s / (nsm * mhz * 1e6),
+                'peak_kind': f'1 shared-memory wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz '
+                             '(median sampled clock)',
+                'traffic': dr4 * ngroups if dr4 else None,
+                'kernel': f'k_osem_batch span 1 (nb_osem_batch_subset, {br.bs} frames per '
+                          f'walk, tile {br.tile}, {ngroups} frame groups per launch)',
+                'wavefronts_per_launch': wl, 'launch_ms_avg': launch_s * 1e3,
+                'hbm': ({'unit': 'GB/s', 'peak': peak, 'peak_kind': peak_kind,
+                         'achieved': dr4 * ngroups / launch_s / 1e9,
+                         'frac': dr4 * ngroups / launch_s / 1e9 / peak} if dr4 else None),
+                'algorithmic': algorithmic}
+    else:
+        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                'frac': achieved / peak, 'traffic': None, 'peak_kind': peak_kind,
+                'kernel': f'k_osem_batch span 1 (nb_osem_batch_subset, {br.bs} frames per '
+                          f'walk, tile {br.tile})',
+                'bytes_per_launch_avg': bytes_iter / len(br.subs),
+                'launch_ms_avg': launch_s * 1e3,
+                'note': 'algorithmic bytes: no capture of this kernel shape in '
+                        'profiles/traffic.json'}
     # e2e: pinned host prompts in, host frames and gradients out
     ph = scan['psng'].cpu().pin_memory()
     img_h = torch.empty((nfr, 320, 320, 127)).pin_memory()
@@ -1299,6 +1347,12 @@ def main():
     ap.add_argument('--hist-steps', type=int, default=10,
                     help='timed steps of the list-mode histogram measured after the batch '
                          'workload (its `hist` sub-object; 0 = skip)')
+    ap.add_argument('--diff-steps', type=int, default=5,
+                    help='timed steps of the differentiable projector measured after the '
+                         'batch workload (its `diff` sub-object; 0 = skip)')
+    ap.add_argument('--dynamic-steps', type=int, default=2,
+                    help='timed steps of the span-1 dynamic frames measured after the batch '
+                         'workload (its `dynamic` sub-object; 0 = skip)')
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if (args.workload == 'hist' and args.impl == 'ours') else 3
@@ -1329,6 +1383,24 @@ def main():
                 'dtype': 'u32', 'config': h['config'], 'roofline': h['roofline'],
                 'cpu_baseline': h.get('cpu_baseline'), 'e2e': h['e2e'],
                 'gpu_launches': h['gpu_launches'], 'clocks': h['clocks']}
+    # the other two batched configurations, measured the same way in the same process
+    subs = {}
+    if args.workload == 'batch':
+        import copy
+        for name, fn, steps in (('diff', run_diff, args.diff_steps),
+                                ('dynamic', run_dynamic, args.dynamic_steps)):
+            if steps <= 0:
+                continue
+            torch.cuda.empty_cache()
+            sa = copy.copy(args)
+            sa.steps, sa.warmup, sa.e2e_steps = steps, 3, 1
+            sa.no_cpu_baseline = True   # the --workload runs carry the CPU baselines
+            r = fn(sa, ws, rank, dev)
+            subs[name] = {'metric': METRIC[name][0], 'value': r['value'],
+                          'unit': METRIC[name][1], 'steps': sa.steps, 'warmup': sa.warmup,
+                          'ms_per_step': r['ms_per_step'], 'dtype': 'f32',
+                          'config': r['config'], 'roofline': r['roofline'], 'e2e': r['e2e'],
+                          'gpu_launches': r['gpu_launches'], 'clocks': r['clocks']}
     metric, unit = METRIC[args.workload]
     if rank == 0:
         line = {'metric': metric, 'value': res['value'], 'unit': unit, 'n_gpus': ws,
@@ -1342,6 +1414,7 @@ def main():
             line['plain_dropin'] = res['plain_dropin']
         if hist is not None:
             line['hist'] = hist
+        line.update(subs)
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -23,6 +23,11 @@ launches 15, 16, 17 are one warm launch of each mode:
 `batch` runs one batched OSEM sub-iteration (subset 0) for 8 images with batch widths 4 and
 2, twice each (capture -k regex:k_osem_batch -s 2 -c 2 for the second launch of each width:
 launches 0, 1 are width 4, 2, 3 width 2 -- use -s 1 -c 1 and -s 3 -c 1).
+
+`diffdyn` launches the projector kernels of the differentiable-projector and dynamic-frame
+workloads twice each: batched forward and back projection of 8 images (span 11, all LORs),
+the attenuation projection, and a span-1 batched OSEM sub-iteration of 4 frames (capture
+-k regex:"k_osem_batch|k_project" -c 8).
 """
 from __future__ import annotations
 
@@ -127,8 +132,50 @@ def sct(device='cuda:0'):
     print('sct ok')
 
 
+def diffdyn(device='cuda:0'):
+    """The projector launches of the differentiable-projector and dynamic-frame workloads,
+    two of each, in this order: the batched forward projection of 8 images (width 4, span
+    11, all 68516 LORs; k_osem_batch forward mode), their batched back projection
+    (backward mode), the attenuation projection of the mu-map (k_project forward), and one
+    span-1 batched OSEM sub-iteration of 4 frames (width 4, subset 0).  About 5 GB on the
+    device.  Capture all eight with
+    -k regex:"k_osem_batch|k_project" -c 8 and a few metrics."""
+    from nipet_b200 import batch as B
+    from nipet_b200 import diffprj, geometry, phantoms
+    dev = torch.device(device)
+    p = geometry.get_mmrparams()
+    gen = torch.Generator(device=dev).manual_seed(1)
+    prj = diffprj.MMRProjector(p, mu=torch.from_numpy(phantoms.water_mumap()), span=11,
+                               device=dev)
+    x = torch.rand((8, 320, 320, 127), device=dev, generator=gen)
+    for _ in range(2):
+        s = prj.project(x)
+    for _ in range(2):
+        prj.backproject(s)
+    del s
+    for _ in range(2):
+        prj.weights()
+    torch.cuda.synchronize(dev)
+    prj.check()
+    del x, prj
+    torch.cuda.empty_cache()
+    nfr = 4
+    y = torch.randint(0, 4, (nfr, 68516, 4084), device=dev, generator=gen,
+                      dtype=torch.int16).view(torch.uint16)
+    an = torch.rand((68516, 4084), device=dev, generator=gen) + 0.5
+    rs = torch.full((68516, 4084), 0.01, device=dev)
+    br = B.BatchRecon(p, y, rs, an, device=dev, span=1, bs=4)
+    br.sens128.fill_(1.0)
+    br.init_images()
+    for _ in range(2):
+        br.subiteration(0)
+    torch.cuda.synchronize(dev)
+    br.geom.check()
+    print('diffdyn ok')
+
+
 if __name__ == '__main__':
-    {'projectors': projectors, 'hist': hist, 'batch': batch, 'sct': sct,
+    {'projectors': projectors, 'hist': hist, 'batch': batch, 'sct': sct, 'diffdyn': diffdyn,
      'hist200': lambda: hist(nwords=200_000_000, duration=600),
      'hist200boot': lambda: hist(nwords=200_000_000, duration=600, nrep=4)}[
         sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
