@@ -129,11 +129,11 @@ static __device__ __forceinline__ EvDec decode_event(int word, const HistLUT &sl
 
 // Add a warp's per-second sums (held per replicate in shared memory) to the global
 // per-second counters and clear them.  Lane l handles replicates l, l + 32, ...
-static __device__ __forceinline__ void flush_seconds(const HistArgs &a, int nrep, uint32_t *acc,
-                                                     int sec, int lane) {
+static __device__ __forceinline__ void flush_seconds(const HistArgs &a, uint32_t *acc, int sec,
+                                                     int lane) {
   __syncwarp();
   if (sec >= 0) {
-    for (int r = lane; r < nrep; r += 32) {
+    for (int r = lane; r < a.nrep; r += 32) {
       uint32_t *q = acc + 3 * r;
       const uint32_t pd = q[0], sz = q[1], sd = q[2];
       const uint32_t sp = pd;
@@ -186,16 +186,11 @@ static __device__ __forceinline__ void second_sums(const HistArgs &a, uint32_t *
 // Persistent: every warp takes the next thread slice from a.next_slice until none is left.
 // Dynamic shared memory: 3 x nrep uint32 per warp (per-second prompt, ring-sum and
 // delayed accumulators of the second the warp is in).
-// ONE: one histogram without bootstrap (nrep 1, btp 0, packed counters), compiled with the
-// replicate loops and the bootstrap / unpacked / bulk paths folded away.
-// (Held to 64 registers for a fourth block per SM the general kernel ran 1.7% slower: 4.20
-// vs 4.13 ms at span 11, 6% more instructions.)
-template <bool ONE>
+// (Held to 64 registers for a fourth block per SM it ran 1.7% slower: 4.20 vs 4.13 ms at
+// span 11, 6% more instructions.  A copy specialised for one histogram without bootstrap
+// -- 32 registers, 6 blocks per SM, 28% fewer instructions -- was slower too, 4.23 ms: the
+// launch waits on its L2 atomics, not on issue.)
 __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
-  const int nrep = ONE ? 1 : a.nrep;
-  const int btp = ONE ? 0 : a.btp;
-  const int unp = ONE ? 0 : a.unp;
-  const int bulk = ONE ? 0 : a.bulk;
   __shared__ HistLUT slut;
   __shared__ uint64_t s_thr[32];
   extern __shared__ uint32_t s_acc[];
@@ -208,8 +203,8 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   const uint4 t4 = make_uint4((uint32_t)a.thr[0], (uint32_t)a.thr[1], (uint32_t)a.thr[2],
                               (uint32_t)a.thr[3]);
   const int lane = threadIdx.x & 31;
-  uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * nrep;
-  for (int r = lane; r < 3 * nrep; r += 32) acc[r] = 0;
+  uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * a.nrep;
+  for (int r = lane; r < 3 * a.nrep; r += 32) acc[r] = 0;
   // bulk mode: two staging rows of rblk weights per thread, after the accumulators (both
   // offsets are multiples of 16 bytes, as the bulk copy needs)
   uint32_t *const stg = s_acc + (size_t)8 * 3 * a.nrep + (size_t)threadIdx.x * 2 * a.rblk;
@@ -219,9 +214,9 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   const int nslices = a.nchnk * NB_TOTHRDS;
   // replicate / bin strides of the two large counter arrays
   // replicate / bin strides of the sinogram counters, the delayed slot offset and shift
-  const size_t pstr_r = unp ? 1 : a.nbins, pstr_b = unp ? 2 * (size_t)a.rblk : 1;
-  const size_t doff = unp ? (size_t)a.rblk : 0;
-  const int dshift = unp ? 0 : 16;
+  const size_t pstr_r = a.unp ? 1 : a.nbins, pstr_b = a.unp ? 2 * (size_t)a.rblk : 1;
+  const size_t doff = a.unp ? (size_t)a.rblk : 0;
+  const int dshift = a.unp ? 0 : 16;
   const size_t sstr_r = (size_t)NB_SEG0 * NB_NSBINANG;
   for (;;) {
     int sl = 0;
@@ -302,7 +297,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           if (lane == L) {
             const unsigned ibck = (unsigned)((word0 & 0x1fffffff) >> 19);
             if (ibck < NB_NBUCKTS) {
-              for (int r = 0; r < nrep; r++) {
+              for (int r = 0; r < a.nrep; r++) {
                 uint32_t *bk = a.bck + (size_t)r * 2 * NB_NBUCKTS * a.nitag;
                 const size_t b0 = ibck + (size_t)NB_NBUCKTS * itag;
                 const size_t b1 = b0 + (size_t)NB_NBUCKTS * a.nitag;
@@ -327,10 +322,10 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
       const int sec0 = __shfl_sync(0xffffffffu, itag, __ffs(evm) - 1);
       const bool uni = __all_sync(0xffffffffu, !evw || itag == sec0);
       if (uni && sec0 != acc_sec) {
-        flush_seconds(a, nrep, acc, acc_sec, lane);
+        flush_seconds(a, acc, acc_sec, lane);
         acc_sec = sec0;
       }
-      if (btp != 1) {
+      if (a.btp != 1) {
         // one decode per word; per replicate only its weight N and the counter updates
         const EvDec e = decode_event(word0, slut, a.span);
         const bool okb = evw && e.valid;
@@ -352,12 +347,12 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         int qblk = -1;
         uint32_t *const row = stg + par * a.rblk;
         // the row's previous bulk add (two steps back) must have read it
-        if (bulk) nb_bulk_wait_read<1>();
+        if (a.bulk) nb_bulk_wait_read<1>();
         bool any = false;
-        for (int r = 0; r < nrep; r++) {
+        for (int r = 0; r < a.nrep; r++) {
           const int rep = a.rep0 + r;
           uint32_t N = 1;
-          if (btp == 2) {
+          if (a.btp == 2) {
             // N ~ Poisson: the number of inverse-CDF thresholds at or below the uniform,
             // output rep % 4 of the Philox block (word index, rep / 4)
             if ((rep >> 2) != qblk) {
@@ -383,14 +378,14 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
             N = k;
           }
           const bool ok = okb && N > 0 && N < 32;
-          if (bulk) {
+          if (a.bulk) {
             row[r] = ok ? N : 0u;
             any |= ok;
           }
           if (ok) {
-            if (!bulk) atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
+            if (!a.bulk) atomicAdd(ps0 + (size_t)r * pstr_r, N << pshift);
             if (e.prompt) {
-              if (!unp) atomicAdd(ss0 + (size_t)r * sstr_r, N);
+              if (!a.unp) atomicAdd(ss0 + (size_t)r * sstr_r, N);
               if (pv) atomicAdd(a.pvs + (size_t)r * a.sne + pvo, N << ((e.an == 126) * 8));
             } else {
               uint32_t *fn = a.fan + (size_t)r * NB_NRINGS * NB_NCRS;
@@ -403,9 +398,9 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           second_sums(a, acc, r, uni, ok, itag, e.prompt ? nn : 0u, e.prompt ? 0u : nn,
                       (ok && e.prompt) ? (uint32_t)e.sis : 0u, lane);
         }
-        if (bulk) {
+        if (a.bulk) {
           // all replicates of the event in one L2 reduction of the bin's replicate block
-          for (int r = nrep; r < a.rblk; r++) row[r] = 0u;
+          for (int r = a.nrep; r < a.rblk; r++) row[r] = 0u;
           if (any) {
             nb_fence_proxy_async_smem();
             nb_bulk_reduce_add_u32(ps0, row, 4u * (uint32_t)a.rblk);
@@ -416,7 +411,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         continue;
       }
       // btp = 1: each replicate replaces the word by a draw from the slice
-      for (int r = 0; r < nrep; r++) {
+      for (int r = 0; r < a.nrep; r++) {
         const int rep = a.rep0 + r;
         int word = word0;
         uint32_t N = 1;
@@ -441,7 +436,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
           if (e.prompt) {
             p_n = N;
             zr = (uint32_t)e.sis;
-            if (!unp)
+            if (!a.unp)
               atomicAdd(a.ssrb + (size_t)r * sstr_r + (size_t)e.sis * NB_NSBINANG + e.aw, N);
             atomicAdd(ps, N);
             if ((e.an == 0 || e.an == 126) && itag < NB_MXNITAG)
@@ -460,9 +455,9 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         second_sums(a, acc, r, uni, ok, itag, p_n, d_n, zr, lane);
       }
     }
-    flush_seconds(a, nrep, acc, acc_sec, lane);
+    flush_seconds(a, acc, acc_sec, lane);
   }
-  if (bulk) nb_bulk_wait_all<0>();
+  if (a.bulk) nb_bulk_wait_all<0>();
 }
 
 // Unpacked scratch [bin][2][rblk] (prompts, delayeds) added into the caller's packed
@@ -649,19 +644,17 @@ static cudaError_t launch_hist(HistArgs &a, unsigned *ctr, cudaStream_t s) {
   int dev = 0, nsm = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const bool one = a.nrep == 1 && a.btp == 0 && !a.unp && !a.bulk;
-  void (*kern)(const HistArgs) = one ? k_hist<true> : k_hist<false>;
   // static plus dynamic shared memory above 48 KB needs the kernel's opt-in
   if (dyn + sizeof(HistLUT) + 32 * sizeof(uint64_t) > 48 * 1024) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
   }
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, dyn);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hist, 256, dyn);
   if (e != cudaSuccess) return e;
   const int nslices = a.nchnk * NB_TOTHRDS;
   int blocks = nsm * (per_sm > 0 ? per_sm : 1);
   if (blocks > (nslices + 7) / 8) blocks = (nslices + 7) / 8;
-  kern<<<blocks, 256, dyn, s>>>(a);
+  k_hist<<<blocks, 256, dyn, s>>>(a);
   return cudaGetLastError();
 }
 
