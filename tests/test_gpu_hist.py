@@ -92,6 +92,32 @@ def test_hist_sparse_tags_and_chunks(params, cuda_device):
     _check(got, ref)
 
 
+def test_span1_slab_counts_fold_to_span11(params, cuda_device):
+    """A span-1 histogram (counted through slab records, one 64 MB slab of counters at a
+    time) of a 30M-word, three-chunk stream over a time window, against the span-11
+    histogram of the same stream (counted directly): the packed span-1 counters summed
+    over the span-1 sinograms of each span-11 sinogram equal the span-11 counters, uint32
+    wrap-around included, and every other output is the same."""
+    lm = phantoms.lm_stream_fast(30_000_000, 60, params=params, seed=4, device=cuda_device)
+    pl = mmr_lmproc.plan(lm.cpu().numpy(), t0=5, t1=50)
+    assert pl['nchnk'] >= 2
+    out = {}
+    for span in (1, 11):
+        Cnt = dict(params['Cnt'], SPN=span, BTP=0)
+        out[span] = mmr_lmproc.hist_stream(lm, params['txLUT'], params['axLUT'], Cnt, t0=5,
+                                           t1=50, pl=pl, unpack=False)
+    p1 = out[1]['psino'].reshape(4084, -1).contiguous().view(torch.int32).to(torch.int64)
+    s11 = torch.from_numpy(np.asarray(params['axLUT']['sn1_sn11'], np.int64)).to(p1.device)
+    fold = torch.zeros((837, p1.shape[1]), dtype=torch.int64, device=p1.device)
+    fold.index_add_(0, s11, p1 & 0xFFFFFFFF)
+    p11 = out[11]['psino'].reshape(837, -1).contiguous().view(torch.int32).to(torch.int64)
+    assert torch.equal(fold & 0xFFFFFFFF, p11 & 0xFFFFFFFF)
+    assert int((p1 & 0xFFFF).sum()) > 0
+    i32 = lambda t: t.view(torch.int32) if t.dtype == torch.uint32 else t  # noqa: E731
+    for k in ('ssr', 'phc', 'dhc', 'zR', 'zM', 'pvs', 'fan', 'bck'):
+        assert torch.equal(i32(out[1][k]), i32(out[11][k])), k
+
+
 def test_lminfo_and_hist_file_api(params, stream, cuda_device, tmp_path):
     f = tmp_path / 'lm.bf'
     stream.tofile(f)
