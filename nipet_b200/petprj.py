@@ -55,6 +55,17 @@ def image_shape_of(Cnt: dict) -> tuple:
     return IMG_SHAPE
 
 
+_SIDE: dict = {}
+
+
+def _side_stream(dev: torch.device) -> torch.cuda.Stream:
+    """A second stream per device, for host-to-device copies that overlap the kernels."""
+    key = str(dev)
+    if key not in _SIDE:
+        _SIDE[key] = torch.cuda.Stream(dev)
+    return _SIDE[key]
+
+
 def _subs_arg(subs, device):
     s = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs).reshape(-1)
     if s.size == 0 or s[0] < 0:
@@ -219,21 +230,51 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     rs = torch.empty((NAW, nsn), device=dev, dtype=torch.float32)
     _lib.check(lib.nb_osem_rs(dev_ptr(rs), dev_ptr(d_r), dev_ptr(d_s) if d_s is not None else None,
                               dev_ptr(d_a), dev_ptr(d_n), NAW * nsn, st))
+    if tuple(np.shape(sensimg)) != (nsub,) + IMG_SHAPE:
+        raise ValueError(f'sensimg must have shape {(nsub,) + IMG_SHAPE}')
     d_img = to_device(img, np.float32, dev)
     img128 = to_col128(d_img)
-    sens = to_device(sensimg, np.float32, dev)
-    if tuple(sens.shape) != (nsub,) + IMG_SHAPE:
-        raise ValueError(f'sensimg must have shape {(nsub,) + IMG_SHAPE}')
-    sens128 = to_col128(sens, nsub)
     m = to_device(msk, np.float32, dev)
     msk128 = (to_col128(m) > 0.5).to(torch.uint8)
     bimg128 = torch.empty_like(img128)
     kp = k.ctypes.data_as(C.c_void_p)
-    if use_psf:
-        work = torch.empty((2, COL128), device=dev, dtype=torch.float32)
-        for i in range(nsub):  # the sensitivity images, convolved once per call
-            _lib.check(lib.nb_psf_col128(dev_ptr(sens128[i]), dev_ptr(sens128[i]), kp,
-                                         dev_ptr(work[0]), st))
+    work = torch.empty((2, COL128), device=dev, dtype=torch.float32) if use_psf else None
+    # The sensitivity images: host float32 images are copied one subset ahead, the next
+    # subset's image staged by the host threads and moved on a side stream while the GPU
+    # runs the current subset (as the reference's call pattern passes them, 14 x 52 MB per
+    # call); anything else in one piece.  Each is convolved once per call with a PSF.
+    staged = (isinstance(sensimg, np.ndarray) and sensimg.dtype == np.float32
+              and sensimg.flags.c_contiguous and nsub >= 2)
+    sens128 = torch.empty((nsub, COL128), device=dev, dtype=torch.float32)
+    if staged:
+        side = _side_stream(dev)
+        tmp = [torch.empty(IMG_SHAPE, device=dev), torch.empty(IMG_SHAPE, device=dev)]
+        freed = [None, None]   # event: the conversion that last read tmp[b] is done
+
+        def prepare(i):
+            b = i & 1
+            if freed[b] is not None:
+                side.wait_event(freed[b])
+            with torch.cuda.stream(side):
+                _lib.check(lib.nb_copy_h2d(dev_ptr(tmp[b]), sensimg[i].ctypes.data_as(
+                    C.c_void_p), sensimg[i].nbytes, C.c_void_p(side.cuda_stream)))
+            copied = torch.cuda.Event()
+            copied.record(side)
+            torch.cuda.current_stream(dev).wait_event(copied)
+            _lib.check(lib.nb_im_to_col128(dev_ptr(sens128[i]), dev_ptr(tmp[b]), 1, st))
+            freed[b] = torch.cuda.Event()
+            freed[b].record(torch.cuda.current_stream(dev))
+            if use_psf:
+                _lib.check(lib.nb_psf_col128(dev_ptr(sens128[i]), dev_ptr(sens128[i]), kp,
+                                             dev_ptr(work[0]), st))
+        prepare(0)
+    else:
+        sens = to_device(sensimg, np.float32, dev)
+        _lib.check(lib.nb_im_to_col128(dev_ptr(sens128), dev_ptr(sens), nsub, st))
+        if use_psf:
+            for i in range(nsub):
+                _lib.check(lib.nb_psf_col128(dev_ptr(sens128[i]), dev_ptr(sens128[i]), kp,
+                                             dev_ptr(work[0]), st))
     for i in range(nsub):
         nprj = int(subs_np[i, 0])
         d_sub = to_device(subs_np[i, 1:1 + nprj].astype(np.int32), np.int32, dev)
@@ -253,6 +294,8 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
                                           dev_ptr(sens128[i]), dev_ptr(msk128),
                                           dev_ptr(d_psng), dev_ptr(rs), dev_ptr(d_sub), nprj,
                                           st))
+        if staged and i + 1 < nsub:
+            prepare(i + 1)
     out = from_col128(img128)
     g.check()
     _writeback(img, out[0])
