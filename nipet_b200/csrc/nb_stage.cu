@@ -17,6 +17,7 @@
 // copy is ordered after the stream's earlier work and the call returns when the host array
 // holds the data; while the host threads unpack one chunk the DMA engine fills the next.
 #include <atomic>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -24,8 +25,8 @@
 
 #include "nb_internal.cuh"
 
-#define NB_STAGE_SLOTS 4
-#define NB_STAGE_CHUNK ((size_t)32 << 20)
+#define NB_STAGE_SLOTS 8
+#define NB_STAGE_CHUNK ((size_t)8 << 20)
 
 namespace {
 
@@ -50,28 +51,93 @@ int stage_init(Stage &s) {
   return NB_OK;
 }
 
-// memcpy of n bytes split over nthr threads (the calling thread takes the last part)
+int copy_threads() {
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int n = hc == 0 ? 4 : (int)hc;
+  return n > 16 ? 16 : n;
+}
+
+// A pool of copy threads, started on first use and kept for the life of the process (they
+// sleep on a condition variable between copies; starting threads for every chunk cost as
+// much as the copy of a small chunk).  run() splits one memcpy into parts, hands them to
+// the workers, copies a part itself and returns when every part is done.  Callers hold
+// their device's staging mutex; the pool serialises callers of different devices.
+class CopyPool {
+ public:
+  explicit CopyPool(int nthr) {
+    for (int t = 0; t < nthr - 1; t++) std::thread([this] { work(); }).detach();
+  }
+  void run(unsigned char *dst, const unsigned char *src, size_t n, int nparts) {
+    std::lock_guard<std::mutex> one(call_mu_);
+    const size_t part = ((n / nparts) + 4095) & ~(size_t)4095;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      dst_ = dst;
+      src_ = src;
+      n_ = n;
+      part_ = part;
+      next_ = 0;
+      left_ = (n + part - 1) / part;
+      ++gen_;
+    }
+    cv_.notify_all();
+    take();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [this] { return left_ == 0; });
+  }
+
+ private:
+  // copy parts until none is left to start
+  void take() {
+    for (;;) {
+      size_t k, off, len;
+      unsigned char *d;
+      const unsigned char *s;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (next_ * part_ >= n_) return;
+        k = next_++;
+        off = k * part_;
+        len = off + part_ < n_ ? part_ : n_ - off;
+        d = dst_;
+        s = src_;
+      }
+      memcpy(d + off, s + off, len);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) done_.notify_all();
+    }
+  }
+  void work() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      take();
+    }
+  }
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_;
+  unsigned char *dst_ = nullptr;
+  const unsigned char *src_ = nullptr;
+  size_t n_ = 0, part_ = 1, next_ = 0, left_ = 0;
+  uint64_t gen_ = 0;
+};
+
+CopyPool &copy_pool() {
+  static CopyPool *p = new CopyPool(copy_threads());  // never destroyed: workers outlive exit
+  return *p;
+}
+
+// memcpy of n bytes split over nthr parts copied by the pool and the calling thread
 void par_copy(unsigned char *dst, const unsigned char *src, size_t n, int nthr) {
   if (nthr <= 1 || n < ((size_t)1 << 20)) {
     memcpy(dst, src, n);
     return;
   }
-  const size_t part = ((n / nthr) + 4095) & ~(size_t)4095;
-  std::vector<std::thread> th;
-  size_t off = 0;
-  for (int t = 0; t < nthr - 1 && off < n; t++) {
-    const size_t len = off + part < n ? part : n - off;
-    th.emplace_back([=] { memcpy(dst + off, src + off, len); });
-    off += len;
-  }
-  if (off < n) memcpy(dst + off, src + off, n - off);
-  for (auto &x : th) x.join();
-}
-
-int copy_threads() {
-  const unsigned hc = std::thread::hardware_concurrency();
-  const int n = hc == 0 ? 4 : (int)hc;
-  return n > 8 ? 8 : n;
+  copy_pool().run(dst, src, n, nthr);
 }
 
 }  // namespace
