@@ -210,7 +210,9 @@ static __device__ __forceinline__ void slab_flush(const HistArgs &a, unsigned *w
   if (c) {
     const unsigned base = wpos[s];
     const unsigned lim = a.roff[(size_t)s * a.nwst + gw + 1];
-    if ((unsigned)lane < c && base + lane < lim) a.rec[base + lane] = wbuf[s * NB_SLAB_CW + lane];
+    // streaming store: the records are read once, by k_slab_add, and should not push the
+    // SSRB counters this launch updates out of L2
+    if ((unsigned)lane < c && base + lane < lim) __stcs(a.rec + base + lane, wbuf[s * NB_SLAB_CW + lane]);
     __syncwarp();
     if (lane == 0) {
       wcnt[s] = 0;
@@ -599,16 +601,16 @@ __global__ void __launch_bounds__(256) k_slab_count(const HistArgs a, unsigned *
       s1 = off + (int64_t)(idx + 1) * e4t;
     }
     if (s1 > off + elm) s1 = off + elm;
-    // four steps of 32 words per iteration, their loads issued together
-    for (int64_t base = s0; base < s1; base += 128) {
-      int w[4];
+    // eight steps of 32 words per iteration, their loads issued together
+    for (int64_t base = s0; base < s1; base += 256) {
+      int w[8];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < 8; k++) {
         const int64_t i = base + 32 * k + lane;
         w[k] = i < s1 ? __ldcs(a.lm + i) : 0;
       }
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < 8; k++) {
         int s = -1;
         if (w[k] > 0) {
           const int val = w[k] & 0x3fffffff;

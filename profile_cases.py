@@ -16,7 +16,9 @@ launches 15, 16, 17 are one warm launch of each mode:
 `hist` histograms a synthetic 20M-word span-11 stream three times (capture -k regex:k_hist -s 2);
 `hist200` does the same on the full-size 2e8-word stream over 600 s (1.2 GB on the device);
 `hist200boot` histograms that stream with 4 Poisson bootstrap replicates per launch (about
-3.4 GB on the device).
+3.4 GB on the device); `hist200s1` histograms it at span 1, through the slab records (about
+3.5 GB on the device; 25 launches per histogram: k_slab_count, k_slab_scan, k_hist and 22
+k_slab_add).
 
 `sct` runs the scatter model twice (capture -k regex:k_sct_psct -s 1 -c 1).
 
@@ -74,13 +76,13 @@ def projectors(device='cuda:0'):
     print('projectors ok')
 
 
-def hist(device='cuda:0', nwords=20_000_000, duration=60, nrep=1):
+def hist(device='cuda:0', nwords=20_000_000, duration=60, nrep=1, span=11):
     from nipet_b200 import geometry, mmr_lmproc, phantoms
     dev = torch.device(device)
     p = geometry.get_mmrparams()
     lm = phantoms.lm_stream_fast(nwords, duration, params=p, seed=0, device=dev)
     pl = mmr_lmproc.plan(lm.cpu().numpy())
-    Cnt = dict(p['Cnt'], SPN=11, BTP=0 if nrep == 1 else 2, BTPRT=1.0)
+    Cnt = dict(p['Cnt'], SPN=span, BTP=0 if nrep == 1 else 2, BTPRT=1.0)
     for _ in range(3):
         r = mmr_lmproc.hist_stream(lm, p['txLUT'], p['axLUT'], Cnt, pl=pl, unpack=False,
                                    nrep=nrep)
@@ -177,5 +179,6 @@ def diffdyn(device='cuda:0'):
 if __name__ == '__main__':
     {'projectors': projectors, 'hist': hist, 'batch': batch, 'sct': sct, 'diffdyn': diffdyn,
      'hist200': lambda: hist(nwords=200_000_000, duration=600),
+     'hist200s1': lambda: hist(nwords=200_000_000, duration=600, span=1),
      'hist200boot': lambda: hist(nwords=200_000_000, duration=600, nrep=4)}[
         sys.argv[1] if len(sys.argv) > 1 else 'projectors']()
