@@ -1002,16 +1002,42 @@ def run_chain(args, ws, rank, dev):
         torch.cuda.synchronize(dev)
         et.append(time.perf_counter() - t)
     te = _max_over_ranks(float(np.mean(et)), ws, dev)
+    # bound of the fused sub-iteration: the shared-memory pipe, with the wavefronts of one
+    # subset launch from the one-kernel capture of the same kernel on a subset of the same
+    # size (profiles/k_project_subset_ncu_full.md); the 14 subsets have equal LOR counts
+    wf = _traffic('osem_subiteration_smem_wavefronts')
+    tr = _traffic('osem_subiteration')
+    algorithmic = {'unit': 'GB/s', 'achieved': achieved, 'frac_of_hbm_peak': achieved / peak,
+                   'bytes_per_launch_avg': float(np.mean(byt)),
+                   'note': '4 B per Siddon voxel read and update as if every one came from '
+                           'HBM, + sinogram rows; above 1 because staged columns are reused '
+                           'from shared memory'}
+    if wf:
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+        la = float(np.mean(dur))
+        roof = {'bound': 'smem', 'achieved': wf / la, 'peak': nsm * mhz * 1e6,
+                'unit': 'wavefronts/s', 'frac': wf / la / (nsm * mhz * 1e6),
+                'peak_kind': f'1 shared-memory wavefront/cycle/SM x {nsm} SMs x {mhz:.0f} MHz '
+                             '(median sampled clock)',
+                'traffic': tr, 'kernel': 'k_project<OSEM> fused sub-iteration inside osemone',
+                'wavefronts_per_launch': wf, 'launch_ms_avg': la * 1e3,
+                'hbm': ({'unit': 'GB/s', 'peak': peak, 'peak_kind': peak_kind,
+                         'achieved': tr / la / 1e9, 'frac': tr / la / 1e9 / peak}
+                        if tr else None),
+                'algorithmic': algorithmic}
+    else:
+        roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                'frac': achieved / peak, 'traffic': tr,
+                'kernel': 'k_project<OSEM> fused sub-iteration inside osemone',
+                'peak_kind': peak_kind, 'bytes_per_launch_avg': float(np.mean(byt)),
+                'launch_ms_avg': float(np.mean(dur)) * 1e3}
     res = {'ms_per_step': t_step * 1e3, 'value': ws / t_step,
            'e2e': {'value': ws / te, 'unit': 'recon/s', 'h2d_bytes_per_step': int(lm_host.nbytes),
                    'd2h_bytes_per_step': int(127 * 344 * 344 * 4),
                    'path': 'mmrhist.hist_device(pinned host words) -> mmrrec.osemone -> host image'},
            'clocks': clocks, 'gpu_launches': CHAIN_LAUNCHES,
-           'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                        'frac': achieved / peak, 'traffic': _traffic('osem_subiteration'),
-                        'kernel': 'k_project<OSEM> fused sub-iteration inside osemone',
-                        'peak_kind': peak_kind, 'bytes_per_launch_avg': float(np.mean(byt)),
-                        'launch_ms_avg': float(np.mean(dur)) * 1e3},
+           'roofline': roof,
            'config': {'workload': f'one frame of the list-mode stream ({lm_host.size} words over '
                                   f'{args.duration} s) through mmrrec.osemone: span-11 histogram, '
                                   'randoms from the delayed fan sums, norm from seeded synthetic '
@@ -1353,6 +1379,9 @@ def main():
     ap.add_argument('--dynamic-steps', type=int, default=2,
                     help='timed steps of the span-1 dynamic frames measured after the batch '
                          'workload (its `dynamic` sub-object; 0 = skip)')
+    ap.add_argument('--chain-steps', type=int, default=3,
+                    help='timed steps of the list-mode-to-image chain (osemone) measured after '
+                         'the batch workload (its `chain` sub-object; 0 = skip)')
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if (args.workload == 'hist' and args.impl == 'ours') else 3
@@ -1388,7 +1417,8 @@ def main():
     if args.workload == 'batch':
         import copy
         for name, fn, steps in (('diff', run_diff, args.diff_steps),
-                                ('dynamic', run_dynamic, args.dynamic_steps)):
+                                ('dynamic', run_dynamic, args.dynamic_steps),
+                                ('chain', run_chain, args.chain_steps)):
             if steps <= 0:
                 continue
             torch.cuda.empty_cache()

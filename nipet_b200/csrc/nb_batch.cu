@@ -706,6 +706,7 @@ extern "C" int nb_osem_batch_subset(nb_geom *g, float *img, float *bimg, const f
                                     const uint8_t *msk128, const uint16_t *psng, const float *rs,
                                     const float *rscale, int nrep, int bs, int tile,
                                     int span, const int32_t *subs, int nprj, void *stream) {
+  NB_RANGE("nb_osem_batch_subset");
   NB_REQUIRE(g != nullptr, "nb_osem_batch_subset: NULL geometry handle");
   NB_REQUIRE(img && bimg && sens128 && msk128 && psng && rs && rscale && subs,
              "nb_osem_batch_subset: NULL argument");
@@ -773,6 +774,7 @@ extern "C" int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128,
                                     const float *sens128, const uint8_t *msk128,
                                     const uint16_t *psng, const float *rs, const int32_t *subs,
                                     int nprj, const float *krnl, float *work128, void *stream) {
+  NB_RANGE("nb_osem_subset_span1");
   NB_REQUIRE(g != nullptr, "nb_osem_subset_span1: NULL geometry handle");
   NB_REQUIRE(img128 && bimg128 && sens128 && msk128 && psng && rs && subs,
              "nb_osem_subset_span1: NULL argument");
@@ -810,6 +812,7 @@ extern "C" int nb_osem_subset_span1(nb_geom *g, float *img128, float *bimg128,
 
 extern "C" int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep, int bs,
                              int span, const int32_t *subs, int nprj, void *stream) {
+  NB_RANGE("nb_fprj_batch");
   NB_REQUIRE(g != nullptr, "nb_fprj_batch: NULL geometry handle");
   NB_REQUIRE(sino && img, "nb_fprj_batch: NULL argument");
   NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_fprj_batch: nrep out of range");
@@ -826,6 +829,7 @@ extern "C" int nb_fprj_batch(nb_geom *g, float *sino, const float *img, int nrep
 
 extern "C" int nb_bprj_batch(nb_geom *g, float *bimg, const float *sino, int nrep, int bs,
                              int span, const int32_t *subs, int nprj, void *stream) {
+  NB_RANGE("nb_bprj_batch");
   NB_REQUIRE(g != nullptr, "nb_bprj_batch: NULL geometry handle");
   NB_REQUIRE(sino && bimg, "nb_bprj_batch: NULL argument");
   NB_REQUIRE(nrep > 0 && nrep <= nbb::NB_MAXREP, "nb_bprj_batch: nrep out of range");

@@ -256,6 +256,7 @@ extern "C" int nb_geom_create(int device, const float *crs, int ncrs, const int1
                               int naw, const float *li2rng, const int16_t *li2sn,
                               const int16_t *li2sn1, const int8_t *li2nos, int nli2r,
                               nb_geom **out) {
+  NB_RANGE("nb_geom_create (Siddon tables, walk checks)");
   NB_REQUIRE(out != nullptr, "nb_geom_create: out is NULL");
   *out = nullptr;
   NB_REQUIRE(crs && s2c && li2rng && li2sn && li2sn1 && li2nos, "nb_geom_create: NULL LUT");

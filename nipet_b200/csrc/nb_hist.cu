@@ -868,6 +868,7 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
                        const int16_t *sn1_rno, const int16_t *s2cF, uint32_t *psino,
                        uint32_t *ssrb, uint32_t *phc, uint32_t *dhc, int32_t *zR, int32_t *zM,
                        uint32_t *pvs, uint32_t *fan, uint32_t *bck, void *stream) {
+  NB_RANGE("nb_hist");
   NB_REQUIRE(lm && atag && ele4chnk && ele4thrd, "nb_hist: NULL stream or plan");
   NB_REQUIRE(sn1_sn11 && sn1_ssrb && sn1_rno && s2cF, "nb_hist: NULL LUT");
   NB_REQUIRE(psino && ssrb && phc && dhc && zR && zM && pvs && fan && bck,
@@ -1076,6 +1077,7 @@ __global__ void k_unpack(const uint32_t *__restrict__ p, size_t n, uint16_t *__r
 
 extern "C" int nb_hist_unpack(const uint32_t *psino, size_t nbins, uint16_t *psn, uint16_t *dsn,
                               unsigned long long *psum, unsigned long long *dsum, void *stream) {
+  NB_RANGE("nb_hist_unpack");
   NB_REQUIRE(psino != nullptr, "nb_hist_unpack: NULL input");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned long long *d = nullptr;

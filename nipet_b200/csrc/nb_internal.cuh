@@ -59,6 +59,17 @@ struct nb_rings {
   int16_t *d_bin1;   // [nrays] ray of each of the range's sinograms
 };
 
+// ---- tracing: an NVTX range around a C-ABI call (header-only NVTX3: without a profiler
+// attached a push / pop costs a branch) ----
+#include <nvtx3/nvToolsExt.h>
+struct NbRange {
+  explicit NbRange(const char *name) { nvtxRangePushA(name); }
+  ~NbRange() { nvtxRangePop(); }
+  NbRange(const NbRange &) = delete;
+  NbRange &operator=(const NbRange &) = delete;
+};
+#define NB_RANGE(name) NbRange nb_range_(name)
+
 // ---- host-side error plumbing (nb_capi.cu) ----
 void nb_set_error_msg(const char *fmt, ...);
 int nb_cuda_fail(cudaError_t e, const char *what, const char *file, int line);

@@ -89,6 +89,7 @@ extern "C" int nb_norm(float *sng, const float *geo, int ngeo, const float *cinf
                        const float *dtp, const float *dtnp, const int32_t *buckets,
                        const int16_t *sn1_rno, const int16_t *sn1_sn11, const int8_t *sn1_sn11no,
                        const int32_t *aw2ali, int span, void *stream) {
+  NB_RANGE("nb_norm");
   NB_REQUIRE(sng && geo && cinf && ceff && axe1 && dtp && dtnp && buckets && sn1_rno &&
                  sn1_sn11 && sn1_sn11no && aw2ali,
              "nb_norm: NULL argument");

@@ -196,6 +196,7 @@ extern "C" int nb_col128_to_im(float *im, const float *im128, int nimg, void *st
 
 extern "C" int nb_fprj_col128(nb_geom *g, float *sino, const float *im128, const int32_t *subs,
                               int nprj, int span, int att, void *stream) {
+  NB_RANGE("nb_fprj");
   int st = check_common(g, nprj, subs, span);
   if (st) return st;
   NB_REQUIRE(sino && im128, "nb_fprj_col128: NULL sino or image");
@@ -209,6 +210,7 @@ extern "C" int nb_fprj_col128(nb_geom *g, float *sino, const float *im128, const
 
 extern "C" int nb_bprj_col128(nb_geom *g, float *im128, const float *sino, const int32_t *subs,
                               int nprj, int span, void *stream) {
+  NB_RANGE("nb_bprj");
   int st = check_common(g, nprj, subs, span);
   if (st) return st;
   NB_REQUIRE(sino && im128, "nb_bprj_col128: NULL sino or image");
@@ -220,6 +222,7 @@ extern "C" int nb_bprj_col128(nb_geom *g, float *im128, const float *sino, const
 
 extern "C" int nb_sens_col128(nb_geom *g, float *sens128, const float *an, const int32_t *subs,
                               int nprj, int span, void *stream) {
+  NB_RANGE("nb_sens");
   int st = check_common(g, nprj, subs, span);
   if (st) return st;
   NB_REQUIRE(sens128 && an, "nb_sens_col128: NULL image or sinogram");
@@ -268,6 +271,7 @@ static int check_rings(nb_geom *g, const nb_rings *rr) {
 
 extern "C" int nb_fprj_rings(nb_geom *g, const nb_rings *rr, float *sino, const float *im,
                              const int32_t *subs, int nprj, int att, void *stream) {
+  NB_RANGE("nb_fprj_rings");
   int st = check_common(g, nprj, subs, 1);
   if (st) return st;
   st = check_rings(g, rr);
@@ -291,6 +295,7 @@ extern "C" int nb_fprj_rings(nb_geom *g, const nb_rings *rr, float *sino, const 
 
 extern "C" int nb_bprj_rings(nb_geom *g, const nb_rings *rr, float *im, const float *sino,
                              const int32_t *subs, int nprj, void *stream) {
+  NB_RANGE("nb_bprj_rings");
   int st = check_common(g, nprj, subs, 1);
   if (st) return st;
   st = check_rings(g, rr);
@@ -325,6 +330,7 @@ extern "C" int nb_osem_rs(float *rs, const float *rsng, const float *ssng, const
 extern "C" int nb_osem_subset(nb_geom *g, float *img128, float *bimg128, const float *sens128,
                               const uint8_t *msk128, const uint16_t *psng, const float *rs,
                               const int32_t *subs, int nprj, void *stream) {
+  NB_RANGE("nb_osem_subset");
   int st = check_common(g, nprj, subs, 11);
   if (st) return st;
   NB_REQUIRE(img128 && bimg128 && sens128 && msk128 && psng && rs && subs,
@@ -356,6 +362,7 @@ extern "C" int nb_osem_subset_psf(nb_geom *g, float *img128, float *bimg128,
                                   const float *sens128, const uint8_t *msk128,
                                   const uint16_t *psng, const float *rs, const int32_t *subs,
                                   int nprj, const float *krnl, float *work128, void *stream) {
+  NB_RANGE("nb_osem_subset_psf");
   int st = check_common(g, nprj, subs, 11);
   if (st) return st;
   NB_REQUIRE(img128 && bimg128 && sens128 && msk128 && psng && rs && subs && krnl && work128,
@@ -425,6 +432,7 @@ __global__ void k_putgaps(float *__restrict__ sino, const float *__restrict__ sn
 
 extern "C" int nb_remgaps(float *sng, const float *sino, int snno, const int32_t *aw2ali,
                           void *stream) {
+  NB_RANGE("nb_remgaps");
   NB_REQUIRE(sng && sino && aw2ali && snno > 0, "nb_remgaps: bad arguments");
   k_remgaps<float><<<2048, 256, 0, (cudaStream_t)stream>>>(sng, sino, snno, aw2ali);
   NB_CUDA(cudaGetLastError());
@@ -441,6 +449,7 @@ extern "C" int nb_remgaps_u16(uint16_t *sng, const uint16_t *sino, int snno,
 
 extern "C" int nb_putgaps(float *sino, const float *sng, int snno, const int32_t *aw2ali,
                           void *stream) {
+  NB_RANGE("nb_putgaps");
   NB_REQUIRE(sng && sino && aw2ali && snno > 0, "nb_putgaps: bad arguments");
   NB_CUDA(cudaMemsetAsync(sino, 0, sizeof(float) * (size_t)snno * NB_NSBINANG,
                           (cudaStream_t)stream));

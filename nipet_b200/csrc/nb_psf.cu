@@ -83,6 +83,7 @@ __global__ void k_psf_xy(float *__restrict__ dst, const float *__restrict__ src,
 
 extern "C" int nb_psf_col128(float *dst128, const float *src128, const float *krnl,
                              float *tmp128, void *stream) {
+  NB_RANGE("nb_psf");
   NB_REQUIRE(dst128 && src128 && krnl && tmp128, "nb_psf_col128: NULL argument");
   NB_REQUIRE(dst128 != tmp128 && src128 != tmp128, "nb_psf_col128: tmp must be its own buffer");
   PsfKernel K;

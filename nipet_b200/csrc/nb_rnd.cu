@@ -104,6 +104,7 @@ extern "C" int nb_randoms(float *rsn, float *cmap, const uint32_t *fansums, cons
                           const int8_t *cij, const int16_t *s2cr, const int16_t *aw2sn,
                           const int16_t *sn1_rno, const int16_t *sn1_sn11, int span, int mrd,
                           void *stream) {
+  NB_RANGE("nb_randoms");
   NB_REQUIRE(rsn && cmap && fansums && crsr && cij && s2cr && aw2sn && sn1_rno,
              "nb_randoms: NULL argument");
   NB_REQUIRE(span == 1 || (span == 11 && sn1_sn11), "nb_randoms: span must be 1 or 11");

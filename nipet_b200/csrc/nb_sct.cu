@@ -368,6 +368,7 @@ extern "C" int nb_sct_vsm(const float *mu, const int8_t *mumsk, const float *em,
                           const int32_t *sctaxR, const float *sctaxW, int nsn64,
                           const int16_t *sn1_sn11, int nsn1, int span, float *sval,
                           float *s3d, int *nvx, void *stream) {
+  NB_RANGE("nb_sct_vsm");
   NB_REQUIRE(mu && mumsk && em && scrs && srng && isrng && knlut && xsxu && offseg && sctaxR &&
                  sctaxW && sn1_sn11 && sval && s3d,
              "nb_sct_vsm: NULL argument");

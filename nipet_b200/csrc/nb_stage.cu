@@ -143,6 +143,7 @@ void par_copy(unsigned char *dst, const unsigned char *src, size_t n, int nthr) 
 }  // namespace
 
 extern "C" int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *stream) {
+  NB_RANGE("nb_copy_h2d");
   NB_REQUIRE(bytes == 0 || (dst && src), "nb_copy_h2d: NULL pointer");
   if (bytes == 0) return NB_OK;
   int dev = 0;
@@ -170,6 +171,7 @@ extern "C" int nb_copy_h2d(void *dst, const void *src, size_t bytes, void *strea
 }
 
 extern "C" int nb_copy_d2h(void *dst, const void *src, size_t bytes, void *stream) {
+  NB_RANGE("nb_copy_d2h");
   NB_REQUIRE(bytes == 0 || (dst && src), "nb_copy_d2h: NULL pointer");
   if (bytes == 0) return NB_OK;
   int dev = 0;
