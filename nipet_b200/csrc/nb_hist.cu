@@ -170,13 +170,13 @@ static __device__ __forceinline__ void second_sums(const HistArgs &a, uint32_t *
                                                    bool uni, bool ok, int itag, uint32_t p_n,
                                                    uint32_t d_n, uint32_t zr, int lane) {
   if (uni) {
-    // prompts and delayeds of the step (each <= 31 x 32) share one reduction
-    const uint32_t spd = __reduce_add_sync(0xffffffffu, p_n | (d_n << 16));
-    const uint32_t sz = __reduce_add_sync(0xffffffffu, zr);
+    // the step's prompts and delayeds (each <= 31 x 32 < 2^10) and ring sums (SSRB index
+    // <= 126, <= 126 x 32 < 2^12) share one 32-bit reduction
+    const uint32_t s = __reduce_add_sync(0xffffffffu, p_n | (d_n << 10) | (zr << 20));
     if (lane == 0) {
-      acc[3 * r] += spd & 0xFFFFu;
-      acc[3 * r + 1] += sz;
-      acc[3 * r + 2] += spd >> 16;
+      acc[3 * r] += s & 0x3FFu;
+      acc[3 * r + 1] += s >> 20;
+      acc[3 * r + 2] += (s >> 10) & 0x3FFu;
     }
     return;
   }
@@ -548,34 +548,48 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
 }
 
 // Unpacked scratch [bin][2][rblk] (prompts, delayeds) added into the caller's packed
-// [nrep][bin] counters: prompts + 65536 x delayeds, the reference's packed uint32 sum
-// (hst.cu:167,192), wrap-around included.
-__global__ void k_pack_add(uint32_t *__restrict__ dst, const uint32_t *__restrict__ src,
-                           size_t nbins, int nrep, int rblk) {
-  for (size_t b = blockIdx.x * (size_t)blockDim.x + threadIdx.x; b < nbins;
-       b += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t *q = src + b * 2 * rblk;
-    for (int r = 0; r < nrep; r++) dst[(size_t)r * nbins + b] += q[r] + (q[rblk + r] << 16);
-  }
-}
-
-// SSRB counters from the unpacked prompts: every output sinogram belongs to one SSRB
-// sinogram (its rings' sum), so SSRB bin (k, aw) of replicate r adds the prompts of bin aw
-// of the sinograms listed in src[off[k] .. off[k+1]).
-__global__ void k_ssrb_derive(uint32_t *__restrict__ ssrb, const uint32_t *__restrict__ src,
-                              const int *__restrict__ off, const int16_t *__restrict__ lst,
-                              int nrep, int rblk) {
+// [nrep][bin] counters -- prompts + 65536 x delayeds, the reference's packed uint32 sum
+// (hst.cu:167,192), wrap-around included -- and the SSRB counters summed from the prompts
+// in the same pass.  Every output sinogram belongs to one SSRB sinogram (its rings' sum),
+// so SSRB bin (k, aw) of replicate r adds the prompts of bin aw of the sinograms listed in
+// lst[off[k] .. off[k+1]); the lists partition the output sinograms, so walking them visits
+// every scratch bin once.  Thread t takes SSRB bin t / ngrp and replicates 4g .. 4g+3,
+// g = t % ngrp (rblk = 4 ngrp): neighbouring threads read neighbouring 16-byte pieces of
+// a bin's block, and each scratch byte is read once.
+__global__ void k_pack_ssrb(uint32_t *__restrict__ dst, uint32_t *__restrict__ ssrb,
+                            const uint32_t *__restrict__ src, const int *__restrict__ off,
+                            const int16_t *__restrict__ lst, size_t nbins, int nrep, int rblk) {
+  const int ngrp = rblk >> 2;
   const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nss;
-       i += (size_t)gridDim.x * blockDim.x) {
+  const size_t nt = nss * ngrp;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nt;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = t / ngrp;
+    const int g = (int)(t - i * ngrp);
     const int k = (int)(i / NB_NSBINANG), aw = (int)(i - (size_t)k * NB_NSBINANG);
-    const int j0 = off[k], j1 = off[k + 1];
-    for (int r = 0; r < nrep; r++) {
-      uint32_t acc = 0;
-      for (int j = j0; j < j1; j++)
-        acc += src[((size_t)lst[j] * NB_NSBINANG + aw) * 2 * rblk + r];
-      ssrb[(size_t)r * nss + i] += acc;
+    const int r0 = 4 * g;
+    uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int j = off[k]; j < off[k + 1]; j++) {
+      const size_t b = (size_t)lst[j] * NB_NSBINANG + aw;
+      const uint32_t *q = src + b * 2 * rblk + r0;
+      // the scratch is read once: streaming loads
+      const uint4 p = __ldcs(reinterpret_cast<const uint4 *>(q));
+      const uint4 d = __ldcs(reinterpret_cast<const uint4 *>(q + rblk));
+      uint32_t *o = dst + (size_t)r0 * nbins + b;
+      o[0] += p.x + (d.x << 16);
+      if (r0 + 1 < nrep) o[nbins] += p.y + (d.y << 16);
+      if (r0 + 2 < nrep) o[2 * nbins] += p.z + (d.z << 16);
+      if (r0 + 3 < nrep) o[3 * nbins] += p.w + (d.w << 16);
+      s0 += p.x;
+      s1 += p.y;
+      s2 += p.z;
+      s3 += p.w;
     }
+    uint32_t *o = ssrb + (size_t)r0 * nss + i;
+    o[0] += s0;
+    if (r0 + 1 < nrep) o[nss] += s1;
+    if (r0 + 2 < nrep) o[2 * nss] += s2;
+    if (r0 + 3 < nrep) o[3 * nss] += s3;
   }
 }
 
@@ -933,6 +947,10 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
                "nb_hist: an output sinogram spans two SSRB sinograms");
     ssrb_of[so] = k;
   }
+  // replicates are packed by walking these lists, which must then reach every sinogram
+  if (nrep > 1)
+    for (int so = 0; so < nout; so++)
+      NB_REQUIRE(ssrb_of[so] >= 0, "nb_hist: an output sinogram lies in no SSRB sinogram");
   std::vector<int> soff(NB_SEG0 + 1, 0);
   std::vector<int16_t> slst;
   for (int k = 0; k < NB_SEG0; k++) {
@@ -1040,8 +1058,7 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && a.unp) {
-    k_pack_add<<<nsm * 8, 256, 0, s>>>(psino, scr, a.nbins, nrep, rblk);
-    k_ssrb_derive<<<nsm * 8, 256, 0, s>>>(ssrb, scr, d_soff, d_slst, nrep, rblk);
+    k_pack_ssrb<<<nsm * 8, 256, 0, s>>>(psino, ssrb, scr, d_soff, d_slst, a.nbins, nrep, rblk);
     e = cudaGetLastError();
   }
   // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go
