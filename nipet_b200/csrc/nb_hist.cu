@@ -23,13 +23,15 @@
 //
 // Performance: persistent warps pull slices from a counter; per-second sums stay in
 // shared memory until the warp's second changes.  With bootstrap replicates nb_hist counts
-// the sinogram unpacked in a scratch ([bin][2][nrep]: prompts and delayeds apart, a bin's
+// the sinogram unpacked in a scratch ([bin][2][rblk]: prompts and delayeds apart, a bin's
 // replicates side by side, so one event's replicate updates share one or two L2
 // sectors), then packs it into the caller's sinograms (prompts + 65536 x delayeds, the
 // reference's uint32 sum) and sums the SSRB counters from the prompts (every output
-// sinogram lies in one SSRB sinogram), so the SSRB counters take no atomics; an event's
-// replicate weights are staged in shared memory and added to its bin's replicate block by
-// one bulk reduce-add (cp.reduce.async.bulk .add.u32) instead of one atomic per replicate.
+// sinogram lies in one SSRB sinogram) in the same pass, so the SSRB counters take no
+// atomics; an event's replicate weights are staged in shared memory and added to its
+// bin's replicate block by one bulk reduce-add (cp.reduce.async.bulk .add.u32) instead of
+// one atomic per replicate.  More than 16 replicates go through in chunks of at most 16,
+// one launch and one scratch fill each.
 // A single span-1 histogram (1.4 GB of counters, ten times L2) writes 4-byte slab records
 // instead of its sinogram atomics and then counts them one 64 MB slab of counters at a
 // time, every update an L2 hit; a single span-11 or SSRB histogram, and nb_hist_static
@@ -88,6 +90,17 @@ struct HistArgs {
 
 #define NB_SLAB_SHIFT 24   // bins per slab: 2^24 uint32 counters = 64 MB, well inside L2
 #define NB_SLAB_CW 32      // records a warp stages per slab before it writes them out
+#define NB_HIST_ROWS 2     // bulk-reduce staging rows per thread, used in turn
+
+// Words between two threads' staging rows: the rows' length rounded up to an odd multiple
+// of four words, so that every row stays 16-byte aligned for the bulk copy and a warp's
+// stores of one replicate's weights spread over 8 banks (4-way, the least any 16-byte
+// stride allows) instead of 1 or 2.
+static __host__ __device__ __forceinline__ int hist_row_stride(int rblk) {
+  const int w = NB_HIST_ROWS * rblk;
+  return ((w >> 2) & 1) ? w : w + 4;
+}
+#define NB_HIST_REPCHUNK 16  // bootstrap replicates per histogram launch, at most
 
 static __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
@@ -262,17 +275,23 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
   for (int i = threadIdx.x; i < (int)(sizeof(HistLUT) / 4); i += blockDim.x)
     reinterpret_cast<int *>(&slut)[i] = reinterpret_cast<const int *>(a.lut)[i];
   if (threadIdx.x < 32) s_thr[threadIdx.x] = a.thr[threadIdx.x];
-  // the first four Poisson thresholds in registers when none is saturated at 2^32 (they
-  // then decide almost every draw)
-  const bool fast4 = a.thr[3] < 4294967296ull;
-  const uint4 t4 = make_uint4((uint32_t)a.thr[0], (uint32_t)a.thr[1], (uint32_t)a.thr[2],
-                              (uint32_t)a.thr[3]);
+  // the first eight Poisson thresholds in registers, less one: x >= thr  <=>  x > thr - 1,
+  // and a threshold saturated at 2^32 becomes 0xFFFFFFFF, which no 32-bit uniform exceeds
+  // (thresholds are ceilings of positive CDF values, so at least 1; the loop over the
+  // shared copy handles a zero).  The first four decide almost every draw, the next four
+  // nearly all the rest.
+  const bool fast = a.thr[0] >= 1;
+  const uint4 t4 = make_uint4((uint32_t)(a.thr[0] - 1), (uint32_t)(a.thr[1] - 1),
+                              (uint32_t)(a.thr[2] - 1), (uint32_t)(a.thr[3] - 1));
+  const uint4 t8 = make_uint4((uint32_t)(a.thr[4] - 1), (uint32_t)(a.thr[5] - 1),
+                              (uint32_t)(a.thr[6] - 1), (uint32_t)(a.thr[7] - 1));
   const int lane = threadIdx.x & 31;
   uint32_t *acc = s_acc + (size_t)(threadIdx.x >> 5) * 3 * a.nrep;
   for (int r = lane; r < 3 * a.nrep; r += 32) acc[r] = 0;
-  // bulk mode: two staging rows of rblk weights per thread, after the accumulators (both
-  // offsets are multiples of 16 bytes, as the bulk copy needs)
-  uint32_t *const stg = s_acc + (size_t)8 * 3 * a.nrep + (size_t)threadIdx.x * 2 * a.rblk;
+  // bulk mode: NB_HIST_ROWS staging rows of rblk weights per thread, after the
+  // accumulators (both offsets are multiples of 16 bytes, as the bulk copy needs)
+  uint32_t *const stg =
+      s_acc + (size_t)8 * 3 * a.nrep + (size_t)threadIdx.x * hist_row_stride(a.rblk);
   // slab records (no bulk staging then): per warp nslab counts, nslab write positions and
   // nslab x CW records
   unsigned *const wcnt =
@@ -286,7 +305,7 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
       wcnt[s] = 0;
       wpos[s] = a.roff[(size_t)s * a.nwst + gw];
     }
-  int par = 0;
+  int par = 0;  // bulk mode: the staging row of the step
   __syncthreads();
 
   const int nslices = a.nchnk * NB_TOTHRDS;
@@ -428,8 +447,9 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
         uint32_t *const ss0 = a.ssrb + sbin;
         uint32_t blk[4] = {0u, 0u, 0u, 0u};
         int qblk = -1;
-        uint32_t *const row = stg + par * a.rblk;
-        // the row's previous bulk add (two steps back) must have read it
+        // the row's previous bulk add (two steps back) must have read it.  (Four rows with
+        // one bulk group per two steps, waiting half as often, ran 22% slower.)
+        uint32_t *const row = stg + (par & 1) * a.rblk;
         if (a.bulk) nb_bulk_wait_read<1>();
         bool any = false;
         for (int r = 0; r < a.nrep; r++) {
@@ -449,11 +469,15 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
             const int j = rep & 3;
             const uint32_t x = j == 0 ? blk[0] : j == 1 ? blk[1] : j == 2 ? blk[2] : blk[3];
             uint32_t k;
-            if (fast4) {
-              k = (uint32_t)(x >= t4.x) + (uint32_t)(x >= t4.y) + (uint32_t)(x >= t4.z) +
-                  (uint32_t)(x >= t4.w);
-              if (k == 4)
-                while (k < 32 && (uint64_t)x >= s_thr[k]) k++;
+            if (fast) {
+              k = (uint32_t)(x > t4.x) + (uint32_t)(x > t4.y) + (uint32_t)(x > t4.z) +
+                  (uint32_t)(x > t4.w);
+              if (k == 4) {
+                k += (uint32_t)(x > t8.x) + (uint32_t)(x > t8.y) + (uint32_t)(x > t8.z) +
+                     (uint32_t)(x > t8.w);
+                if (k == 8)
+                  while (k < 32 && (uint64_t)x >= s_thr[k]) k++;
+              }
             } else {
               k = 0;
               while (k < 32 && (uint64_t)x >= s_thr[k]) k++;
@@ -833,7 +857,7 @@ extern "C" int nb_hist_trim(void) {
 // dynamic shared memory of a k_hist launch: per-second sums, bulk staging rows, slab records
 static size_t hist_dyn(const HistArgs &a, bool slab) {
   return (size_t)8 * 3 * a.nrep * sizeof(uint32_t) +
-         (a.bulk ? (size_t)256 * 2 * a.rblk * sizeof(uint32_t) : 0) +
+         (a.bulk ? (size_t)256 * hist_row_stride(a.rblk) * sizeof(uint32_t) : 0) +
          (slab ? (size_t)8 * a.nslab * (NB_SLAB_CW + 2) * sizeof(uint32_t) : 0);
 }
 
@@ -1000,17 +1024,17 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
   // scratch, then packed into the caller's sinograms, and the SSRB counters are summed
   // from the prompts instead of counted per event.  One histogram counts both directly
   // (an unpacked scratch would double its L2 footprint for less than it saves).
+  // Replicates go through in chunks of at most NB_HIST_REPCHUNK, as equal as possible (the
+  // staging rows of a chunk must fit in shared memory, and the scratch is sized for one).
   uint32_t *scr = nullptr;
-  const int rblk = (nrep + 3) & ~3;
-  const size_t scr_bytes = sizeof(uint32_t) * a.nbins * 2 * (size_t)rblk;
+  const int nrch = (nrep + NB_HIST_REPCHUNK - 1) / NB_HIST_REPCHUNK;
+  const int rchunk = (nrep + nrch - 1) / nrch;
+  const size_t scr_bytes = sizeof(uint32_t) * a.nbins * 2 * (size_t)((rchunk + 3) & ~3);
   if (e == cudaSuccess && nrep > 1) {
     e = cudaMallocFromPoolAsync((void **)&scr, scr_bytes, pool, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(scr, 0, scr_bytes, s);
     if (e == cudaSuccess) {
       a.unp = 1;
-      a.rblk = rblk;
       a.bulk = 1;
-      a.psino = scr;
     }
   }
   // One histogram without bootstrap whose sinogram counters are larger than L2: its events
@@ -1051,15 +1075,41 @@ extern "C" int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t 
       a.roff = roff;
     }
   }
-  if (e == cudaSuccess) e = launch_hist(a, ctr, s);
-  if (e == cudaSuccess && a.rec) {
-    for (int sl = 0; sl < nslab; sl++)
-      k_slab_add<<<nsm * 8, 256, 0, s>>>(psino, rec, a.roff, sl, a.nwst);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess && a.unp) {
-    k_pack_ssrb<<<nsm * 8, 256, 0, s>>>(psino, ssrb, scr, d_soff, d_slst, a.nbins, nrep, rblk);
-    e = cudaGetLastError();
+  if (a.unp) {
+    // one launch per replicate chunk, its outputs at the chunk's first replicate, its
+    // replicate numbers (the random streams) from rep0 + c0
+    const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
+    for (int c0 = 0; c0 < nrep && e == cudaSuccess; c0 += rchunk) {
+      const int nc = nrep - c0 < rchunk ? nrep - c0 : rchunk;
+      const int rblk = (nc + 3) & ~3;
+      HistArgs ac = a;
+      ac.rep0 = rep0 + c0;
+      ac.nrep = nc;
+      ac.rblk = rblk;
+      ac.psino = scr;
+      ac.ssrb = ssrb + c0 * nss;
+      ac.phc = phc + (size_t)c0 * nitag;
+      ac.dhc = dhc + (size_t)c0 * nitag;
+      ac.zR = zR + (size_t)c0 * nitag;
+      ac.zM = zM + (size_t)c0 * nitag;
+      ac.pvs = pvs + c0 * a.sne;
+      ac.fan = fan + (size_t)c0 * NB_NRINGS * NB_NCRS;
+      ac.bck = bck + (size_t)c0 * 2 * NB_NBUCKTS * nitag;
+      e = cudaMemsetAsync(scr, 0, sizeof(uint32_t) * a.nbins * 2 * (size_t)rblk, s);
+      if (e == cudaSuccess) e = launch_hist(ac, ctr, s);
+      if (e == cudaSuccess) {
+        k_pack_ssrb<<<nsm * 8, 256, 0, s>>>(psino + c0 * a.nbins, ac.ssrb, scr, d_soff, d_slst,
+                                            a.nbins, nc, rblk);
+        e = cudaGetLastError();
+      }
+    }
+  } else {
+    if (e == cudaSuccess) e = launch_hist(a, ctr, s);
+    if (e == cudaSuccess && a.rec) {
+      for (int sl = 0; sl < nslab; sl++)
+        k_slab_add<<<nsm * 8, 256, 0, s>>>(psino, rec, a.roff, sl, a.nwst);
+      e = cudaGetLastError();
+    }
   }
   // a pageable-source cudaMemcpyAsync has staged `h` before returning, so `h` may go
   if (rec) cudaFreeAsync(rec, s);

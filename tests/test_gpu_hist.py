@@ -79,6 +79,24 @@ def test_hist_ten_replicates(params, stream, cuda_device, span):
                 for k, v in got.items()}, ref)
 
 
+@pytest.mark.parametrize('btp,nrep,check', [(2, 37, (0, 12, 13, 25, 26, 36)),
+                                             (1, 18, (0, 8, 9, 17))])
+def test_hist_replicates_in_chunks(params, stream, cuda_device, btp, nrep, check):
+    """More replicates than one launch takes (16): they go through in equal chunks (37 as
+    13 + 13 + 11, 18 as 9 + 9), each chunk's outputs at its first replicate and its
+    random streams from its own replicate numbers.  The first and last replicate of every
+    chunk are checked against the oracle."""
+    Cnt = dict(params['Cnt'], SPN=11, BTP=btp, BTPRT=1.0)
+    got = mmr_lmproc.hist_stream(stream, params['txLUT'], params['axLUT'], Cnt, nrep=nrep,
+                                 rep0=3, seed=5)
+    for r in check:
+        ref = O.hist(stream, params, span=11, btp=btp, btprt=1.0, seed=5, rep=3 + r)
+        _check({k: (v[r] if isinstance(v, torch.Tensor) and v.dim() > 0 and k != 'plan' else v)
+                for k, v in got.items()}, ref)
+    del got
+    torch.cuda.empty_cache()
+
+
 def test_hist_sparse_tags_and_chunks(params, cuda_device):
     """Tags every 50 ms with many events between them: thread slices without a time tag
     (the reference then attributes them to second `nitag`, i.e. drops them), and a stream
