@@ -364,7 +364,8 @@ def run_batch(args, ws, rank, dev):
     # back-projection update per image, the images' prompt rows (2 B) and one (r+s)/(an)
     # and a*n row per image group (4 B each)
     _, per_lor = br.geom.count_reads(per_lor=True)
-    ngroups = (nrep + br.bs - 1) // br.bs
+    ngroups = sum(p.ngroups for p in br.parts)
+    slots = sum(p.ngroups * p.bs for p in br.parts)   # images walked, padding included
     bytes_sub = [nrep * 8 * int(per_lor[s.cpu().numpy()].sum()) +
                  br.nprj * NSN11 * (2 * nrep + 8 * ngroups) for s in br.subs]
     bytes_iter = float(sum(bytes_sub))
@@ -414,15 +415,20 @@ def run_batch(args, ws, rank, dev):
     t_launch = t_it / len(br.subs)
     achieved_alg = bytes_iter / t_it / 1e9
     peak, peak_kind = _peaks()
-    gscale = ngroups / 2.0 if br.bs == 4 else None
+    # the 8-image capture walks 8 image slots; a narrower tail launch is scaled the same
+    # way, per image slot (its per-image shared traffic is that of width 4 within a few %)
+    gscale = slots / 8.0 if br.bs == 4 else None
     tr8 = _traffic('osem_batch_8img')
     wf8 = _traffic('osem_batch_8img_smem_wavefronts')
     traffic = None if (tr8 is None or gscale is None) else tr8 * gscale
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
     smem_peak = nsm * mhz * 1e6
+    tail = (f' + {br.parts[1].n} at width {br.parts[1].bs} in a second launch'
+            if len(br.parts) > 1 else '')
     kernel = (f'k_osem_batch (nb_osem_batch_subset, {br.bs} images per walk, tile {br.tile}, '
-              f'{ngroups} image groups per launch)')
+              f'{br.parts[0].ngroups} image groups per launch{tail}; a launch here is one '
+              'sub-iteration)')
     if wf8 and gscale is not None:
         wf = wf8 * gscale
         roof = {'bound': 'smem', 'achieved': wf / t_launch, 'peak': smem_peak,
@@ -666,7 +672,7 @@ def run_dynamic(args, ws, rank, dev):
     # per-launch algorithmic bytes of k_osem_batch at span 1 (as in the batch workload:
     # 8 B per voxel read/update per frame, prompt rows and one (r+s)/(an), a*n row per group)
     _, per_lor = br.geom.count_reads(per_lor=True)
-    ngroups = (nfr + br.bs - 1) // br.bs
+    ngroups = sum(p.ngroups for p in br.parts)
     bytes_iter = float(sum(nfr * 8 * int(per_lor[sb.cpu().numpy()].sum()) +
                            br.nprj * 4084 * (2 * nfr + 8 * ngroups) for sb in br.subs))
 

@@ -22,7 +22,7 @@ from .device import dev_ptr, get_geometry, stream_ptr
 from .mmrrec import subset_table
 from .petprj import COL128, to_col128
 
-__all__ = ['BatchRecon', 'autotune', 'bootstrap_prompts']
+__all__ = ['BatchRecon', 'autotune', 'bootstrap_prompts', 'split_parts']
 
 NAW = 68516
 _TUNE_CACHE: dict = {}
@@ -40,13 +40,41 @@ def bootstrap_prompts(mean: torch.Tensor, totals, seed: int = 0) -> torch.Tensor
     return out
 
 
+def split_parts(nrep: int, bs: int, split_tail: bool = True) -> list[tuple[int, int, int]]:
+    """(first image, images, width) of the launches one sub-iteration makes.  nrep images
+    at width bs leave nrep % bs of them in a last group that walks padding images too; with
+    `split_tail` that remainder gets a launch of its own at the smallest width that holds
+    it (1 or 2; a remainder of 3 at width 4 keeps the padded group)."""
+    rem = nrep % bs
+    if not split_tail or rem == 0 or nrep < bs:
+        return [(0, nrep, bs)]
+    w = 1 if rem == 1 else (2 if rem == 2 else 4)
+    if w >= bs:
+        return [(0, nrep, bs)]
+    return [(0, nrep - rem, bs), (nrep - rem, rem, w)]
+
+
+class _Part:
+    """Images [r0, r0 + n) in the batched layout of width bs."""
+
+    def __init__(self, r0: int, n: int, bs: int, device):
+        self.r0, self.n, self.bs = r0, n, bs
+        self.ngroups = (n + bs - 1) // bs
+        self.img = torch.empty(self.ngroups * COL128 * bs, device=device)
+        self.bimg = torch.zeros_like(self.img)
+
+
 class BatchRecon:
-    """OSEM for `nrep` images on one device (span 11 or 1, PSF off)."""
+    """OSEM for `nrep` images on one device (span 11 or 1, PSF off).  The images go
+    through `bs` at a time; a remainder of nrep % bs images is reconstructed by a second,
+    narrower launch per sub-iteration (`split_parts`) rather than as a padded group."""
 
     def __init__(self, params: dict, psng: torch.Tensor, rs: torch.Tensor, an: torch.Tensor,
                  rscale=None, device=None, span: int = 11, bs: int | None = None,
-                 nsub: int = 14, mask_radius: float = 29.0, tile: int | None = None):
+                 nsub: int = 14, mask_radius: float = 29.0, tile: int | None = None,
+                 split_tail: bool = True):
         self.device = torch.device(device or psng.device)
+        self.split_tail = bool(split_tail)
         self.params = params
         self.span = int(span)
         self.nout = 837 if self.span == 11 else 4084
@@ -78,9 +106,9 @@ class BatchRecon:
         self._alloc()
 
     def _alloc(self):
-        ng = (self.nrep + self.bs - 1) // self.bs
-        self.img = torch.empty(ng * COL128 * self.bs, device=self.device)
-        self.bimg = torch.zeros_like(self.img)
+        self.parts = None  # the previous shape's buffers go first
+        self.parts = [_Part(r0, n, w, self.device)
+                      for r0, n, w in split_parts(self.nrep, self.bs, self.split_tail)]
         self.graph = None
 
     # -------------------------------------------------------------------------------------
@@ -93,18 +121,22 @@ class BatchRecon:
             self.launches += 1
 
     def init_images(self, value: float = 1.0):
-        """Every image set to `value` in place, in the batched layout (one fill kernel)."""
-        _lib.check(self.lib.nb_fill_batch(dev_ptr(self.img), float(value), self.nrep, self.bs,
-                                          stream_ptr(self.device)))
-        self.launches += 1
+        """Every image set to `value` in place, in the batched layout (one fill kernel per
+        part)."""
+        for p in self.parts:
+            _lib.check(self.lib.nb_fill_batch(dev_ptr(p.img), float(value), p.n, p.bs,
+                                              stream_ptr(self.device)))
+            self.launches += 1
 
     def subiteration(self, i: int, stream=None):
         st = stream if stream is not None else stream_ptr(self.device)
-        _lib.check(self.lib.nb_osem_batch_subset(
-            self.geom.handle, dev_ptr(self.img), dev_ptr(self.bimg), dev_ptr(self.sens128[i]),
-            dev_ptr(self.msk128), dev_ptr(self.psng), dev_ptr(self.rs), dev_ptr(self.rscale),
-            self.nrep, self.bs, self.tile, self.span, dev_ptr(self.subs[i]), self.nprj, st))
-        self.launches += 2
+        for p in self.parts:
+            _lib.check(self.lib.nb_osem_batch_subset(
+                self.geom.handle, dev_ptr(p.img), dev_ptr(p.bimg), dev_ptr(self.sens128[i]),
+                dev_ptr(self.msk128), dev_ptr(self.psng[p.r0]), dev_ptr(self.rs),
+                dev_ptr(self.rscale[p.r0:]), p.n, p.bs, self.tile, self.span,
+                dev_ptr(self.subs[i]), self.nprj, st))
+            self.launches += 2
 
     def iteration(self, use_graph: bool = True):
         """One OSEM iteration (all subsets) for all images; replayed from a CUDA graph after
@@ -119,10 +151,11 @@ class BatchRecon:
             s.wait_stream(torch.cuda.current_stream(self.device))
             g = torch.cuda.CUDAGraph()
             with torch.cuda.stream(s):
-                snap = self.img.clone()
+                snap = [p.img.clone() for p in self.parts]
                 for i in range(self.nsub):
                     self.subiteration(i, C_stream(s))
-                self.img.copy_(snap)
+                for p, x in zip(self.parts, snap):
+                    p.img.copy_(x)
                 del snap
                 with torch.cuda.graph(g, stream=s):
                     for i in range(self.nsub):
@@ -130,7 +163,7 @@ class BatchRecon:
             torch.cuda.current_stream(self.device).wait_stream(s)
             self.graph = g
         self.graph.replay()
-        self.launches += 2 * self.nsub
+        self.launches += 2 * self.nsub * len(self.parts)
 
     def run(self, niter: int = 4, use_graph: bool = True, with_sensitivity: bool = True):
         if with_sensitivity:
@@ -142,8 +175,9 @@ class BatchRecon:
 
     def images(self) -> torch.Tensor:
         out = torch.empty((self.nrep, 320, 320, 127), device=self.device)
-        _lib.check(self.lib.nb_from_batch(dev_ptr(out), dev_ptr(self.img), self.nrep, self.bs,
-                                          stream_ptr(self.device)))
+        for p in self.parts:
+            _lib.check(self.lib.nb_from_batch(dev_ptr(out[p.r0]), dev_ptr(p.img), p.n, p.bs,
+                                              stream_ptr(self.device)))
         return out
 
     def mean_std(self, distributed: bool = False, group=None):

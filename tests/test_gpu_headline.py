@@ -3,10 +3,11 @@
 The headline workload reconstructs bootstrap replicates of uneven count levels together:
 4 images per walk of the geometry (`k_osem_batch`, batch width 4), 4 iterations x the
 reference's 14 subsets over all 68,516 LORs, span 11, 320 x 320 x 127.  Here 9 replicates
-(so the last group of 4 is padded) -- 7 at 3e7 counts and 2 at 3e6 counts, in different
-groups, each with its own randoms level -- are reconstructed with the default tile and
-with the shape the autotuner picks, and compared with the FP64 oracle's restatement of
-`recon.cu:318-497` run on the same inputs:
+-- 7 at 3e7 counts and 2 at 3e6 counts, in different groups, each with its own randoms
+level -- are reconstructed with the default tile (two groups of 4 and the ninth replicate
+in a second launch at width 1, as the benchmark's 50 replicates run 48 + 2), with the
+ninth in a padded third group of 4 instead, and with the shape the autotuner picks, and
+compared with the FP64 oracle's restatement of `recon.cu:318-497` run on the same inputs:
 
 * every image within 1e-4 relative L2 inside the mask;
 * the voxel-wise mean and standard deviation (ddof 1) over the replicates within 1e-4
@@ -94,9 +95,16 @@ def _check_against_oracle(got, H, what):
 
 
 def test_batched_width4_default_tile_matches_oracle(params, cuda_device, headline):
+    assert batch.split_parts(len(TOTALS), 4) == [(0, 8, 4), (8, 1, 1)]
     got, shape = _batched(params, headline, cuda_device, bs=4, tile=0)
     assert shape == (4, 0)
-    _check_against_oracle(got, headline, 'width 4, tile 0')
+    _check_against_oracle(got, headline, 'width 4 + tail at width 1, tile 0')
+
+
+def test_batched_width4_padded_group_matches_oracle(params, cuda_device, headline):
+    got, shape = _batched(params, headline, cuda_device, bs=4, tile=0, split_tail=False)
+    assert shape == (4, 0)
+    _check_against_oracle(got, headline, 'width 4, padded last group, tile 0')
 
 
 def test_batched_autotuned_shape_matches_oracle(params, cuda_device, headline, tmp_path,
