@@ -577,28 +577,32 @@ __global__ void __launch_bounds__(256) k_hist(const HistArgs a) {
 // in the same pass.  Every output sinogram belongs to one SSRB sinogram (its rings' sum),
 // so SSRB bin (k, aw) of replicate r adds the prompts of bin aw of the sinograms listed in
 // lst[off[k] .. off[k+1]); the lists partition the output sinograms, so walking them visits
-// every scratch bin once.  Thread t takes SSRB bin t / ngrp and replicates 4g .. 4g+3,
-// g = t % ngrp (rblk = 4 ngrp): neighbouring threads read neighbouring 16-byte pieces of
-// a bin's block, and each scratch byte is read once.
+// every scratch bin once.  A warp takes 32 consecutive SSRB bins and one group of four
+// replicates, 4g .. 4g+3 (rblk = 4 ngrp), the ngrp warps of the other groups of the same
+// bins next to it: the sinogram stores of a warp are whole 128-byte lines, and the
+// 16-byte pieces of a bin's block that one warp skips are read by its neighbours while the
+// lines are still in L1 (cached loads; streaming loads, or one thread per bin and group,
+// measured 1.2 and 0.9 ms slower at 10 replicates x 72.6M bins).
 __global__ void k_pack_ssrb(uint32_t *__restrict__ dst, uint32_t *__restrict__ ssrb,
                             const uint32_t *__restrict__ src, const int *__restrict__ off,
                             const int16_t *__restrict__ lst, size_t nbins, int nrep, int rblk) {
   const int ngrp = rblk >> 2;
   const size_t nss = (size_t)NB_SEG0 * NB_NSBINANG;
-  const size_t nt = nss * ngrp;
+  const size_t nt = ((nss + 31) / 32) * 32 * ngrp;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nt;
        t += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = t / ngrp;
-    const int g = (int)(t - i * ngrp);
+    const size_t wid = t >> 5;
+    const size_t i = (wid / ngrp) * 32 + (t & 31);
+    const int g = (int)(wid % ngrp);
+    if (i >= nss) continue;
     const int k = (int)(i / NB_NSBINANG), aw = (int)(i - (size_t)k * NB_NSBINANG);
     const int r0 = 4 * g;
     uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     for (int j = off[k]; j < off[k + 1]; j++) {
       const size_t b = (size_t)lst[j] * NB_NSBINANG + aw;
       const uint32_t *q = src + b * 2 * rblk + r0;
-      // the scratch is read once: streaming loads
-      const uint4 p = __ldcs(reinterpret_cast<const uint4 *>(q));
-      const uint4 d = __ldcs(reinterpret_cast<const uint4 *>(q + rblk));
+      const uint4 p = __ldg(reinterpret_cast<const uint4 *>(q));
+      const uint4 d = __ldg(reinterpret_cast<const uint4 *>(q + rblk));
       uint32_t *o = dst + (size_t)r0 * nbins + b;
       o[0] += p.x + (d.x << 16);
       if (r0 + 1 < nrep) o[nbins] += p.y + (d.y << 16);
