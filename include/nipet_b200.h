@@ -267,7 +267,13 @@ int nb_lm_plan(const int32_t *lm, int64_t ele, int t0, int t1, int cap, int64_t 
  *   pvs [nrep][sne] uint32, fan [nrep][64*504] uint32, bck [nrep][2*224*nitag] uint32
  *   (nbins: 354033792 span 1, 72557856 span 11, 11009376 span 0;
  *    sne = ceil(min(nitag,5400)/4)*127*344 as lmproc.cu:60-63)
- *   sn1_sn11, sn1_ssrb, sn1_rno, s2cF: host LUTs (axLUT/txLUT, int16). */
+ *   sn1_sn11, sn1_ssrb, sn1_rno, s2cF: host LUTs (axLUT/txLUT, int16).
+ * Device scratch comes stream-ordered from the histogrammer's own memory pool, which keeps
+ * it for the next call (nb_hist_trim releases it).  With nrep > 1 the replicates go through
+ * in equal launches of at most 16, each counting into an unpacked scratch of
+ * nbins * 8 * r bytes (r: the launch's replicates rounded up to a multiple of 4; 7.0 GB for
+ * 10 replicates at span 11); one span-1 histogram without bootstrap takes 4 bytes per
+ * stream word of slab records. */
 int nb_hist(const int32_t *lm, int64_t ele, int nchnk, const int64_t *atag, const int *ele4chnk,
             const int *ele4thrd, int toff, int nitag, int tstart, int tstop, int span, int btp,
             double btprt, uint64_t seed, int rep0, int nrep, const int16_t *sn1_sn11,
