@@ -92,6 +92,14 @@ class Clocks:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # nvidia-smi's start-up (driver and NVML initialisation) competes with the GPU work
+        # for about a second: let it finish (its first sample written) before the timed
+        # region, or a short launch-bound step pays for it
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < 5.0:
+            if self.p.poll() is not None or os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:
