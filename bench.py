@@ -215,7 +215,7 @@ def cpu_hist_sample(lm, params, seconds=10.0):
 def run_osem(args, ws, rank, dev):
     import torch
     from nipet_b200 import _lib, geometry, mmrrec, petprj
-    from nipet_b200.device import dev_ptr, stream_ptr
+    from nipet_b200.device import stream_ptr
 
     params = geometry.get_mmrparams()
     Cnt = dict(params['Cnt'], DEVID=dev.index)

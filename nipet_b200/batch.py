@@ -5,10 +5,10 @@ per-subset sensitivity images; each has its own prompts and a randoms level
 (`rscale[b]` times a common (r+s)/(an) sinogram).  One sub-iteration of all images is one
 persistent kernel launch (`nb_osem_batch_subset`) -- two when the images left over by the
 batch width go through a narrower launch of their own (`split_parts`) -- and a full
-iteration (14 sub-iterations) can be captured once as a CUDA graph and replayed.  The batch width `bs` (images sharing
-one walk of the Siddon geometry) and the kernel's tile shape (columns of the LOR staged
-per shared-memory chunk, rays per thread) are chosen by `autotune`, which times the
-candidates on the device and caches the choice per device.
+iteration (14 sub-iterations) can be captured once as a CUDA graph and replayed.  The
+batch width `bs` (images sharing one walk of the Siddon geometry) and the kernel's tile
+shape (columns of the LOR staged per shared-memory chunk, rays per thread) are chosen by
+`autotune`, which times the candidates on the device and caches the choice per device.
 """
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ import torch
 from . import _lib, geometry
 from .device import dev_ptr, get_geometry, stream_ptr
 from .mmrrec import subset_table
-from .petprj import COL128, to_col128
+from .petprj import COL128
 
 __all__ = ['BatchRecon', 'autotune', 'bootstrap_prompts', 'split_parts']
 

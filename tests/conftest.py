@@ -3,7 +3,6 @@ everything else runs on the CPU (oracle, host logic, C-ABI symbol checks)."""
 import os
 import sys
 
-import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

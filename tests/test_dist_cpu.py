@@ -2,7 +2,6 @@
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 from nipet_b200.shard import replicate_range
