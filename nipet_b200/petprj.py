@@ -213,15 +213,32 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     use_psf = k.size > 0 and k[0] >= 0
     if use_psf and k.size != 3 * 17:
         raise ValueError('krnl must have shape (3, 17)')
-    g = get_geometry(txLUT, axLUT, dev)
+    # every shape is checked before any device work: the kernels index these arrays by
+    # the sizes the span and the subsets imply
     nsn = 837 if span == 11 else 4084
+    subs_np = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs)
+    if subs_np.ndim != 2 or subs_np.shape[0] < 1:
+        raise ValueError('subs must have shape (Nsub, 1 + Nprj) with subs[i, 0] = Nprj')
+    nsub = subs_np.shape[0]
+    counts = subs_np[:, 0].astype(np.int64)
+    if (counts < 1).any() or (counts > subs_np.shape[1] - 1).any():
+        raise ValueError('subs[i, 0] must be the number of LOR indices that follow it in row i')
+    for i in range(nsub):
+        row = subs_np[i, 1:1 + counts[i]]
+        if row.min() < 0 or row.max() >= NAW:
+            raise ValueError(f'subset {i}: LOR index out of range [0, {NAW})')
+    for a, nm in ((psng, 'psng'), (rsng, 'rsng'), (ssng, 'ssng'), (nsng, 'nsng'),
+                  (asng, 'asng')):
+        if a is not None and tuple(np.shape(a)) != (NAW, nsn):
+            raise ValueError(f'{nm} must have shape {(NAW, nsn)}')
+    if tuple(np.shape(sensimg)) != (nsub,) + IMG_SHAPE:
+        raise ValueError(f'sensimg must have shape {(nsub,) + IMG_SHAPE}')
+    for a, nm in ((img, 'img'), (msk, 'msk')):
+        if tuple(np.shape(a)) != IMG_SHAPE:
+            raise ValueError(f'{nm} must have shape {IMG_SHAPE}')
+    g = get_geometry(txLUT, axLUT, dev)
     lib = _lib.load()
     st = stream_ptr(dev)
-    subs_np = np.asarray(subs.cpu() if isinstance(subs, torch.Tensor) else subs)
-    nsub = subs_np.shape[0]
-    for a, nm in ((psng, 'psng'), (rsng, 'rsng'), (nsng, 'nsng'), (asng, 'asng')):
-        if tuple(np.shape(a)) != (NAW, nsn):
-            raise ValueError(f'{nm} must have shape {(NAW, nsn)}')
     d_psng = to_device(psng, np.uint16, dev)
     d_r = to_device(rsng, np.float32, dev)
     d_s = to_device(ssng, np.float32, dev) if ssng is not None else None
@@ -230,8 +247,6 @@ def osem(img, psng, rsng, ssng, nsng, asng, subs, sensimg, msk, krnl, txLUT, axL
     rs = torch.empty((NAW, nsn), device=dev, dtype=torch.float32)
     _lib.check(lib.nb_osem_rs(dev_ptr(rs), dev_ptr(d_r), dev_ptr(d_s) if d_s is not None else None,
                               dev_ptr(d_a), dev_ptr(d_n), NAW * nsn, st))
-    if tuple(np.shape(sensimg)) != (nsub,) + IMG_SHAPE:
-        raise ValueError(f'sensimg must have shape {(nsub,) + IMG_SHAPE}')
     d_img = to_device(img, np.float32, dev)
     img128 = to_col128(d_img)
     m = to_device(msk, np.float32, dev)

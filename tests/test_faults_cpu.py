@@ -1,7 +1,7 @@
 """Faults made on the host, as a user's bad inputs make them: a truncated or tag-less
-list-mode file, an empty stream, LUTs of the wrong size.  Each must end in a Python
-exception with a clear message (the reference calls exit() on such inputs), before any
-GPU work -- so these run without a GPU."""
+list-mode file, an empty stream, LUTs of the wrong size, OSEM inputs of mismatched
+shapes.  Each must end in a Python exception with a clear message (the reference calls
+exit() on such inputs), before any GPU work -- so these run without a GPU."""
 import ctypes as C
 
 import numpy as np
@@ -55,3 +55,37 @@ def test_geometry_with_wrong_lut_sizes_is_refused(ncrs, naw, nli2r, what):
         _lib.call('nb_geom_create', 0, p(crs), ncrs, p(s2c), naw, p(li2rng), p(li2sn),
                   p(li2sn), p(li2nos), nli2r, C.byref(h))
     assert not h.value
+
+
+def _osem_args(params, span=11, **over):
+    """petprj.osem arguments of the right shapes that hold no memory (broadcast zeros);
+    `over` replaces some of them."""
+    nsn = 837 if span == 11 else 4084
+    z = lambda shape, dt=np.float32: np.broadcast_to(np.zeros((), dt), shape)  # noqa: E731
+    subs = np.zeros((14, 1 + 4894), np.int32)
+    subs[:, 0] = 4894
+    a = dict(img=z((320, 320, 127)), psng=z((68516, nsn), np.uint16), rsng=z((68516, nsn)),
+             ssng=z((68516, nsn)), nsng=z((68516, nsn)), asng=z((68516, nsn)), subs=subs,
+             sensimg=z((14, 320, 320, 127)), msk=z((320, 320, 127), np.bool_),
+             krnl=np.full((3, 17), -1, np.float32), txLUT=params['txLUT'],
+             axLUT=params['axLUT'], cnst=dict(params['Cnt'], SPN=span))
+    a.update(over)
+    return a
+
+
+@pytest.mark.parametrize('span,over,what', [
+    (1, {'ssng': np.broadcast_to(np.float32(0), (68516, 837))}, 'ssng must have shape'),
+    (11, {'img': np.broadcast_to(np.float32(0), (320, 320, 126))}, 'img must have shape'),
+    (11, {'msk': np.broadcast_to(np.bool_(0), (344, 344, 127))}, 'msk must have shape'),
+    (11, {'sensimg': np.broadcast_to(np.float32(0), (13, 320, 320, 127))}, 'sensimg must'),
+    (11, {'subs': np.full((14, 11), 20, np.int32)}, r'subs\[i, 0\]'),
+    (11, {'subs': np.array([[2, 5, 68516]], np.int32)}, 'out of range'),
+    (11, {'subs': np.arange(10, dtype=np.int32)}, 'subs must have shape'),
+])
+def test_osem_refuses_mismatched_inputs_before_device_work(params, span, over, what):
+    """A scatter sinogram of the other span, a short image or mask, too few sensitivity
+    images or a subset table whose counts exceed its rows would make the kernels read past
+    their buffers: petprj.osem raises before it touches the device."""
+    from nipet_b200 import petprj
+    with pytest.raises(ValueError, match=what):
+        petprj.osem(**_osem_args(params, span, **over))
