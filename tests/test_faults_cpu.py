@@ -89,3 +89,24 @@ def test_osem_refuses_mismatched_inputs_before_device_work(params, span, over, w
     from nipet_b200 import petprj
     with pytest.raises(ValueError, match=what):
         petprj.osem(**_osem_args(params, span, **over))
+
+
+def test_hist_replicates_need_every_sinogram_in_an_ssrb_list(params):
+    """Bootstrap replicates are packed into the caller's sinograms by walking each SSRB
+    sinogram's list of output sinograms; axial LUTs that leave an output sinogram out of
+    every list (here every span-1 sinogram mapped to span-11 sinogram 0) are refused
+    before any GPU work.  The device pointers are never dereferenced."""
+    lm = phantoms.lm_stream(20_000, 3, seed=2, params=params)
+    pl = mmr_lmproc.plan(lm)
+    hp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    atag = np.ascontiguousarray(pl['atag'], np.int64)
+    e4c = np.ascontiguousarray(pl['ele4chnk'], np.int32)
+    e4t = np.ascontiguousarray(pl['ele4thrd'], np.int32)
+    zeros = np.zeros(4084, np.int16)
+    rno = np.zeros(2 * 4084, np.int16)
+    s2c = np.zeros((86688, 2), np.int16)
+    fake = C.c_void_p(256)
+    with pytest.raises(_lib.NBError, match='lies in no SSRB sinogram'):
+        _lib.call('nb_hist', fake, lm.size, pl['nchnk'], hp(atag), hp(e4c), hp(e4t), pl['toff'],
+                  pl['nitag'], pl['tstart'], pl['tstop'], 11, 2, 1.0, 7, 0, 2, hp(zeros),
+                  hp(zeros), hp(rno), hp(s2c), *([fake] * 9), None)
