@@ -78,18 +78,33 @@ class BatchRecon:
         self.split_tail = bool(split_tail)
         self.params = params
         self.span = int(span)
+        if self.span not in (1, 11):
+            raise ValueError(f'span must be 1 or 11, got {span}')
+        if bs and int(bs) not in (1, 2, 4):
+            raise ValueError(f'bs must be 1, 2 or 4, got {bs}')
+        if tile is not None and int(tile) not in TILES:
+            raise ValueError(f'tile must be one of {TILES}, got {tile}')
         self.nout = 837 if self.span == 11 else 4084
-        self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
-        self.lib = _lib.load()
         dev = self.device
         if psng.dtype != torch.uint16 or psng.dim() != 3 or tuple(psng.shape[1:]) != (NAW,
                                                                                       self.nout):
             raise ValueError(f'psng must be uint16 [nrep, {NAW}, {self.nout}]')
+        for t, nm in ((rs, 'rs'), (an, 'an')):
+            if tuple(t.shape) != (NAW, self.nout):
+                raise ValueError(f'{nm} must have shape {(NAW, self.nout)}')
+        nrep = int(psng.shape[0])
+        if nrep < 1:
+            raise ValueError('psng holds no image')
+        if rscale is not None and np.asarray(rscale).reshape(-1).size != nrep:
+            raise ValueError(f'rscale must hold one value per image ({nrep})')
+        self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
+        self.lib = _lib.load()
         self.psng = psng.to(dev).contiguous()
-        self.nrep = int(psng.shape[0])
+        self.nrep = nrep
         self.rs = rs.to(dev, torch.float32).contiguous()
         self.an = an.to(dev, torch.float32).contiguous()
-        rsc = np.ones(self.nrep, np.float32) if rscale is None else np.asarray(rscale, np.float32)
+        rsc = (np.ones(self.nrep, np.float32) if rscale is None
+               else np.asarray(rscale, np.float32).reshape(-1))
         self.rscale = torch.from_numpy(rsc).to(dev)
         tab = subset_table(params, nsub)
         self.nsub, self.nprj = tab.shape[0], int(tab[0, 0])

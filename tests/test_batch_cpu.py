@@ -22,3 +22,32 @@ def test_split_parts(nrep, bs, parts):
 
 def test_split_parts_off():
     assert split_parts(50, 4, split_tail=False) == [(0, 50, 4)]
+
+
+def _zeros(shape, dtype=None):
+    """A tensor of the given shape that holds no memory (an expanded scalar)."""
+    import torch
+    return torch.zeros((), dtype=dtype or torch.float32).expand(*shape)
+
+
+@pytest.mark.parametrize('kw,what', [
+    ({'span': 1}, r'psng must be uint16 \[nrep, 68516, 4084\]'),
+    ({'rs': (68516, 4084)}, 'rs must have shape'),
+    ({'an': (68516, 836)}, 'an must have shape'),
+    ({'rscale': [1.0, 1.0, 1.0]}, 'one value per image'),
+    ({'bs': 3}, 'bs must be 1, 2 or 4'),
+    ({'tile': 5}, 'tile must be one of'),
+    ({'span': 0}, 'span must be 1 or 11'),
+])
+def test_batch_recon_refuses_mismatched_inputs(params, kw, what):
+    """Inputs the batched kernels would index past their ends (a randoms or a*n sinogram
+    of the other span, a randoms scale per image missing) are refused before any device
+    work, so this runs without a GPU."""
+    import torch
+
+    from nipet_b200 import batch
+    psng = _zeros((2, 68516, 837), torch.uint16)
+    rs = _zeros(kw.pop('rs', (68516, 837)))
+    an = _zeros(kw.pop('an', (68516, 837)))
+    with pytest.raises(ValueError, match=what):
+        batch.BatchRecon(params, psng, rs, an, **kw)
