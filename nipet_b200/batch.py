@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib, geometry
-from .device import dev_ptr, get_geometry, stream_ptr
+from .device import dev_ptr, get_geometry, resolve_device, stream_ptr
 from .mmrrec import subset_table
 from .petprj import COL128
 
@@ -74,7 +74,7 @@ class BatchRecon:
                  rscale=None, device=None, span: int = 11, bs: int | None = None,
                  nsub: int = 14, mask_radius: float = 29.0, tile: int | None = None,
                  split_tail: bool = True):
-        self.device = torch.device(device or psng.device)
+        self.device = resolve_device(device if device is not None else psng.device)
         self.split_tail = bool(split_tail)
         self.params = params
         self.span = int(span)

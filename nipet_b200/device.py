@@ -13,12 +13,22 @@ import torch
 from . import _lib
 
 __all__ = ['Geometry', 'get_geometry', 'to_device', 'dev_ptr', 'stream_ptr', 'device_of',
-           'projector', 'RingSet', 'get_rings', 'full_axial_lut', 'is_reduced']
+           'resolve_device', 'projector', 'RingSet', 'get_rings', 'full_axial_lut',
+           'is_reduced']
+
+
+def resolve_device(device=None) -> torch.device:
+    """`device` (default 'cuda') with an explicit index: 'cuda' alone means the current
+    CUDA device, so that tensors on it compare equal and geometry handles are shared."""
+    d = torch.device(device if device is not None else 'cuda')
+    if d.type == 'cuda' and d.index is None:
+        d = torch.device('cuda', torch.cuda.current_device())
+    return d
 
 
 def device_of(Cnt: dict | None = None, device=None) -> torch.device:
     if device is not None:
-        return torch.device(device)
+        return resolve_device(device)
     idx = int(Cnt.get('DEVID', 0)) if Cnt else 0
     return torch.device('cuda', idx)
 
@@ -135,6 +145,7 @@ _LOCK = threading.Lock()
 def get_geometry(txLUT: dict, axLUT: dict, device: torch.device) -> Geometry:
     """The geometry handle for these LUTs on `device` (built on first use, then cached --
     the reference rebuilds its tables on every call)."""
+    device = resolve_device(device)
     key = (str(device), id(txLUT['crs']), id(txLUT['s2c']), id(axLUT['li2rng']),
            id(axLUT['li2sn']), id(axLUT['li2sn1']), id(axLUT['li2nos']))
     with _LOCK:

@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import dev_ptr, get_geometry, stream_ptr, to_device
+from .device import dev_ptr, get_geometry, resolve_device, stream_ptr, to_device
 
 __all__ = ['MMRProjector', 'ForwardProjection', 'poisson_nll']
 
@@ -48,7 +48,7 @@ class MMRProjector:
                  device=None):
         if span not in (1, 11):
             raise ValueError('span must be 1 or 11')
-        self.device = torch.device(device or 'cuda')
+        self.device = resolve_device(device)
         self.span = int(span)
         self.nsn = 837 if span == 11 else 4084
         self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
@@ -84,6 +84,10 @@ class MMRProjector:
     def project(self, x: torch.Tensor, att: int = 0) -> torch.Tensor:
         """A x for [B, 320, 320, 127] x (att=1: exp(-A x), the attenuation factors).  Batches
         of two or more emission images share each walk of the geometry (nb_fprj_batch)."""
+        if (x.dim() != 4 or tuple(x.shape[1:]) != IMG_SHAPE or x.dtype != torch.float32
+                or x.device != self.device or not x.is_contiguous()):
+            raise ValueError(f'images must be contiguous float32 [B, *{IMG_SHAPE}] tensors on '
+                             f'{self.device}')
         B = x.shape[0]
         out = torch.empty((B, self.nprj, self.nsn), device=self.device)
         st = stream_ptr(self.device)
@@ -103,6 +107,11 @@ class MMRProjector:
 
     def backproject(self, s: torch.Tensor) -> torch.Tensor:
         """A^T s for [B, nprj, nsinos] s (batches of two or more: nb_bprj_batch)."""
+        if (s.dim() != 3 or tuple(s.shape[1:]) != (self.nprj, self.nsn)
+                or s.dtype != torch.float32 or s.device != self.device
+                or not s.is_contiguous()):
+            raise ValueError(f'sinograms must be contiguous float32 [B, {self.nprj}, '
+                             f'{self.nsn}] tensors on {self.device}')
         B = s.shape[0]
         out = torch.empty((B,) + IMG_SHAPE, device=self.device)
         st = stream_ptr(self.device)

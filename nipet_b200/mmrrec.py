@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib, geometry, phantoms
-from .device import dev_ptr, device_of, get_geometry, stream_ptr
+from .device import dev_ptr, device_of, get_geometry, resolve_device, stream_ptr
 from .geometry import get_subsets14
 from .petprj import COL128, from_col128, to_col128
 
@@ -176,7 +176,7 @@ class Recon:
                       (ssng, 'ssng')):
             if a is not None and tuple(np.shape(a)) != (NAW, self.nsn):
                 raise ValueError(f'{nm} must have shape {(NAW, self.nsn)} at span {self.span}')
-        self.device = torch.device(device or 'cuda')
+        self.device = resolve_device(device)
         self.params = params
         self.geom = get_geometry(params['txLUT'], params['axLUT'], self.device)
         self.lib = _lib.load()
