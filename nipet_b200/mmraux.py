@@ -58,6 +58,9 @@ def remgaps(sino, txLUT, Cnt, output=None):
     dev = device_of(Cnt)
     is_np = not isinstance(sino, torch.Tensor)
     arr = np.asarray(sino) if is_np else sino
+    # the kernel reads 252 x 344 bins of every sinogram
+    if arr.ndim < 2 or arr.shape[0] < 1 or int(np.prod(tuple(arr.shape[1:]))) != 252 * 344:
+        raise ValueError(f'sino must have shape (nsinos, 252, 344), got {tuple(arr.shape)}')
     nsn = int(arr.shape[0])
     u16 = (arr.dtype == np.uint16) if is_np else (arr.dtype == torch.uint16)
     dt = np.uint16 if u16 else np.float32
@@ -84,6 +87,11 @@ def putgaps(s, txLUT, Cnt, sino_no=0):
     arr = np.asarray(s) if is_np else s
     nsn = int(sino_no) if sino_no > 0 else (nsinos_for(Cnt) if arr.ndim != 2 else
                                             int(arr.shape[1]))
+    # the kernel reads the gap-free layout [68516][nsn]
+    size = int(np.prod(tuple(arr.shape)))
+    if size != 68516 * nsn:
+        raise ValueError(f'a gap-free sinogram of {nsn} sinograms has 68516 x {nsn} bins, '
+                         f'got shape {tuple(arr.shape)}')
     d_in = to_device(arr, np.float32, dev)
     out = torch.empty((nsn, 252, 344), device=dev, dtype=torch.float32)
     _lib.check(_lib.load().nb_putgaps(dev_ptr(out), dev_ptr(d_in), nsn,

@@ -110,3 +110,19 @@ def test_hist_replicates_need_every_sinogram_in_an_ssrb_list(params):
         _lib.call('nb_hist', fake, lm.size, pl['nchnk'], hp(atag), hp(e4c), hp(e4t), pl['toff'],
                   pl['nitag'], pl['tstart'], pl['tstop'], 11, 2, 1.0, 7, 0, 2, hp(zeros),
                   hp(zeros), hp(rno), hp(s2c), *([fake] * 9), None)
+
+
+@pytest.mark.parametrize('shape', [(837, 252, 343), (837,), (0, 252, 344)])
+def test_remgaps_refuses_a_sinogram_of_the_wrong_shape(params, shape):
+    from nipet_b200 import mmraux
+    with pytest.raises(ValueError, match=r'\(nsinos, 252, 344\)'):
+        mmraux.remgaps(np.broadcast_to(np.float32(0), shape), params['txLUT'], params['Cnt'])
+
+
+@pytest.mark.parametrize('shape,sino_no', [((68516, 836), 837), ((68515, 837), 0),
+                                           ((68516, 837), 100)])
+def test_putgaps_refuses_a_sinogram_of_the_wrong_size(params, shape, sino_no):
+    from nipet_b200 import mmraux
+    with pytest.raises(ValueError, match='gap-free sinogram'):
+        mmraux.putgaps(np.broadcast_to(np.float32(0), shape), params['txLUT'], params['Cnt'],
+                       sino_no=sino_no)
