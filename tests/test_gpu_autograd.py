@@ -126,7 +126,8 @@ def test_batch_of_8_matches_single_images(params, cuda_device, weights_in):
         (g1,) = torch.autograd.grad(l1, x1)
         # the batch shares each walk of the geometry over 4 images (nb_fprj_batch /
         # nb_bprj_batch); one image goes through nb_fprj / nb_bprj: equal to rounding
-        assert abs(float(l1) - float(loss[b])) <= 1e-6 * abs(float(l1))
+        l1v, lbv = float(l1.detach()), float(loss[b].detach())
+        assert abs(l1v - lbv) <= 1e-6 * abs(l1v)
         rl2 = float(torch.linalg.vector_norm(g1 - gb[b]) / torch.linalg.vector_norm(g1))
         assert rl2 <= 1e-5, rl2
     prj.check()
